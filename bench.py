@@ -1,0 +1,340 @@
+# SPDX-License-Identifier: 0BSD
+"""Benchmark of the FP64 z-averaged heat step on B200.
+
+Workload (one GPU): 8192 x 8192 nodes, dx = 5 um, k = 20 W/m/K, rho = 7900,
+cp = 500, 50 um layer, absorptivity 0.4, 200 W, r0 = 50 um, dt = 0.2 dx^2/alpha,
+bidirectional raster (100 um hatch, 1 m/s, 10 tracks over 20000 steps), mirror
+edges, reference loss terms, uniform 300 K start.  One bench step = 1000 time
+steps of the plan (the plan continues across bench steps; 20 bench steps = the
+full 20000-step run).  Metric: GCell-updates/s (cells x time steps / second).
+
+Arms:
+  --impl b200       (default) liblpbf_b200 through its C-ABI; `value` is timed
+                    with the fields resident in HBM, `e2e` through the public
+                    call on pinned host buffers (field in, field + per-step
+                    Partials out, every bench step).
+  --impl reference  the reference's own CPU step task (StepTileTask, compiled
+                    from the reference sources into oracle/_ref and driven by
+                    the hh-compat graph over ny/64 row strips on all host
+                    threads), on a bounded prefix of the same workload.
+
+Multi-GPU (torchrun): every rank advances its own independent 8192^2 field
+(raster angle differs by rank); no data-path collective; weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_SIDE = 8192
+N_STEPS_TOTAL = 20000
+STEPS_PER_ITER = 1000
+BYTES_PER_UPDATE = 16          # read T (8 B) + write T (8 B) per cell-update
+
+
+def workload(rank: int = 0):
+    from hedgehog_lpbf_b200 import params as P
+    from hedgehog_lpbf_b200 import plan as PL
+    mat, pr = P.benchmark_material_process()
+    dom = P.square_domain(N_SIDE)
+    dt = P.dt_fraction(mat, dom)
+    k = P.make_const(mat, pr, dom, dt)
+    angle = np.deg2rad(15.0 * rank)
+    plan = PL.raster_for_steps(dom, dt, N_STEPS_TOTAL, V=1.0, hatch=100e-6, n_tracks=10,
+                               angle=angle)
+    return mat, pr, dom, k, plan
+
+
+def plan_slice(plan, i):
+    idx = (np.arange(STEPS_PER_ITER) + i * STEPS_PER_ITER) % len(plan)
+    return plan[idx]
+
+
+def config(depth, n_gpus):
+    return {"workload": f"{N_SIDE}x{N_SIDE} FP64 z-averaged heat step, bidirectional raster "
+                        "(100 um hatch, 1 m/s, 10 tracks / 20000 steps), dx 5 um, mirror edges",
+            "grid": [N_SIDE, N_SIDE], "time_steps_per_bench_step": STEPS_PER_ITER,
+            "temporal_depth": depth, "parallelism": f"independent fields x{n_gpus}",
+            "l2": "inputs larger than L2 (two 537 MB f64 fields per GPU)"}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(depth):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/advance_kernel_8192.md), or None."""
+    p = os.path.join(ROOT, "profiles", "advance_kernel_8192.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith(f"traffic_per_launch_bytes_depth{depth}"):
+            return float(line.split("=")[1].split()[0])
+    return None
+
+
+class ClockSampler:
+    """Samples SM clocks and clock-event reasons through NVML every 100 ms."""
+
+    REASONS = {
+        "gpu_idle": 0x1, "applications_clocks_setting": 0x2, "sw_power_cap": 0x4,
+        "hw_slowdown": 0x8, "sync_boost": 0x10, "sw_thermal_slowdown": 0x20,
+        "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80,
+        "display_clock_setting": 0x100,
+    }
+
+    def __init__(self, index: int):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+        self.t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, bit in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self._stop.wait(0.1)
+
+    def __enter__(self):
+        if self.nv:
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self.nv and self.t.is_alive():
+            self.t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons - {"gpu_idle"}), "samples": len(self.samples)}
+
+
+def cpu_reference_rate(mat, pr, dom, k, plan, budget_s: float, threads: int | None = None):
+    """GCell-updates/s of the reference CPU path on a bounded prefix."""
+    from oracle import oracle as O
+    from hedgehog_lpbf_b200 import plan as PL
+    las = PL.laser_array(plan)
+    n_threads = threads or os.cpu_count() or 1
+    T = np.full(dom.nx * dom.ny, pr.Tamb)
+    if O.have_reference():
+        kind = "reference"
+        _, w1, _ = O.ref_hh_run(T, mat, pr, dom, k.dt, las[:1], n_threads, dom.ny // 64, Tm=mat.Tm)
+        n = int(max(1, min(len(las) - 1, budget_s / max(w1, 1e-3))))
+        T, wall, _ = O.ref_hh_run(T, mat, pr, dom, k.dt, las[1:1 + n], n_threads, dom.ny // 64,
+                                  Tm=mat.Tm)
+        cores = n_threads
+        desc = (f"reference StepTileTask (hh-compat graph, {dom.ny // 64} row strips, "
+                f"{n_threads} threads) + its per-step driver work, {n} steps of {dom.nx}x{dom.ny}")
+    else:
+        kind = "port"
+        t0 = time.perf_counter()
+        O.run(T, k, las[:1], Tm=mat.Tm, with_ring=False)
+        w1 = time.perf_counter() - t0
+        n = int(max(1, min(len(las) - 1, budget_s / max(w1, 1e-3))))
+        t0 = time.perf_counter()
+        O.run(T, k, las[1:1 + n], Tm=mat.Tm)
+        wall = time.perf_counter() - t0
+        cores = 1
+        desc = f"oracle C port (single thread), {n} steps of {dom.nx}x{dom.ny}"
+    rate = dom.nx * dom.ny * n / wall / 1e9
+    return {"value": rate, "unit": "GCell-updates/s", "cores": cores, "kind": kind,
+            "sample": desc, "wall_s": wall}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    mat, pr, dom, k, plan = workload(0)
+    per_step = []
+    for _ in range(args.warmup):
+        cpu_reference_rate(mat, pr, dom, k, plan, budget_s=1.0)
+    for _ in range(args.steps):
+        per_step.append(cpu_reference_rate(mat, pr, dom, k, plan, budget_s=args.ref_budget))
+    rate = statistics.median(r["value"] for r in per_step)
+    cb = dict(per_step[-1])
+    cb["value"] = rate
+    wall = sum(r["wall_s"] for r in per_step)
+    line = {"metric": "GCell-updates/s", "value": rate, "unit": "GCell-updates/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * wall / max(1, len(per_step)), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "config": config(None, args.gpus), "cpu_baseline": cb,
+            "e2e": {"value": rate, "unit": "GCell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200_arm(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from hedgehog_lpbf_b200.solver import Solver
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    mat, pr, dom, k, plan = workload(rank)
+    s = Solver(k, device=dev, Tm=mat.Tm, depth=args.depth)
+    depth = min(4, args.depth) if args.depth > 0 else (4 if N_SIDE * N_SIDE >= (1 << 22) else 2)
+    launches = s.launches(STEPS_PER_ITER)
+    ring = s.new_ring(STEPS_PER_ITER)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up
+    for i in range(args.warmup):
+        s.advance(plan_slice(plan, i), ring)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    step_ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        step_ev[0].record(stream)
+        for i in range(args.steps):
+            s.advance(plan_slice(plan, args.warmup + i), ring)
+            step_ev[i + 1].record(stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    step_ms = [step_ev[i].elapsed_time(step_ev[i + 1]) for i in range(args.steps)]
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    err = s.read_error()
+
+    cells = dom.nx * dom.ny
+    updates = cells * STEPS_PER_ITER * args.steps * world
+    value = updates / (ms_max * 1e-3) / 1e9
+
+    # ---- end-to-end through the public call, host buffers -----------------
+    host_in = torch.full((dom.ny, dom.nx), 300.0, dtype=torch.float64).pin_memory()
+    host_out = torch.empty((dom.ny, dom.nx), dtype=torch.float64).pin_memory()
+    host_ring = torch.empty(STEPS_PER_ITER * 24, dtype=torch.uint8).pin_memory()
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(e2e_steps):
+        s.field.copy_(host_in, non_blocking=True)
+        s.advance(plan_slice(plan, i), ring)
+        host_out.copy_(s.field, non_blocking=True)
+        host_ring.copy_(ring, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t2 = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_value = cells * STEPS_PER_ITER * e2e_steps * world / (float(t2.item()) * 1e-3) / 1e9
+
+    if rank != 0:
+        return
+    peak, peak_src = measured_peaks()
+    launch_ms = statistics.median(step_ms) / launches
+    steps_per_launch = STEPS_PER_ITER / launches
+    achieved = BYTES_PER_UPDATE * cells * steps_per_launch / (launch_ms * 1e-3) / 1e9
+    traffic = profile_traffic(depth)
+    line = {
+        "metric": "GCell-updates/s", "value": value, "unit": "GCell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (uniform 300 K start, seeded raster plan per rank)",
+        "config": config(depth, world),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
+                     "kernel": f"advance_kernel<{depth},TMA,reduce>",
+                     "algorithmic_bytes": f"{BYTES_PER_UPDATE} B per cell-update x {cells} cells"
+                                          f" x {steps_per_launch:g} steps per launch",
+                     "launch_ms": launch_ms},
+        "e2e": {"value": e2e_value, "unit": "GCell-updates/s",
+                "h2d_bytes_per_step": cells * 8,
+                "d2h_bytes_per_step": cells * 8 + STEPS_PER_ITER * 24,
+                "steps": e2e_steps},
+        "gpu_launches": launches * args.steps,
+        "clocks": clk.summary(),
+        "error_word": err,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_reference_rate(mat, pr, dom, k, plan, budget_s=args.ref_budget)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--depth", type=int, default=0, help="time steps per launch (0 = auto)")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--ref-budget", type=float, default=15.0,
+                    help="seconds of CPU work per reference sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_b200_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

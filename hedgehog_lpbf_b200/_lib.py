@@ -1,0 +1,92 @@
+# SPDX-License-Identifier: 0BSD
+"""ctypes binding of liblpbf_b200.so (the C-ABI of include/lpbf_kernels.hpp
+and include/lpbf_b200.h).
+
+The library is built in-tree by ``hedgehog_lpbf_b200.build``.  There is no
+fallback: if the library cannot be built or loaded, ``lib()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+from . import build as _build
+from .params import Partial, StepConst, Tick
+
+_lock = threading.Lock()
+_lib = None
+
+LPBF_OK = 0
+_vp = ctypes.c_void_p
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class Opts(ctypes.Structure):
+    """lpbf_b200_opts (include/lpbf_b200.h)."""
+    _fields_ = [("phys", ctypes.c_int), ("bc", ctypes.c_int), ("T_edge", ctypes.c_double),
+                ("Tm", ctypes.c_double), ("depth", ctypes.c_int), ("rows", ctypes.c_int)]
+
+
+# name -> (restype, argtypes); every symbol the headers in include/ declare.
+SIGNATURES = {
+    # include/lpbf_kernels.hpp (reference drop-in)
+    "lpbf_launch_step": (None, [_vp, _vp, ctypes.POINTER(StepConst), ctypes.c_int, _vp]),
+    "lpbf_launch_reduce": (None, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _vp,
+                                  ctypes.c_int, _vp]),
+    "lpbf_launch_step_reduce": (None, [_vp, _vp, ctypes.POINTER(StepConst), ctypes.c_int,
+                                       ctypes.c_double, _vp, _vp]),
+    "lpbf_launch_reduce_finalize": (None, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+                                           _vp]),
+    "lpbf_launch_extract_col": (None, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
+    # include/lpbf_b200.h
+    "lpbf_b200_version": (ctypes.c_int, []),
+    "lpbf_b200_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "lpbf_b200_workspace_bytes": (ctypes.c_size_t, []),
+    "lpbf_b200_workspace_init": (ctypes.c_int, [_vp, ctypes.c_size_t, _vp]),
+    "lpbf_b200_advance": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(StepConst), _vp, ctypes.c_int,
+                                         ctypes.POINTER(Opts), _vp, _vp, ctypes.c_size_t, _vp,
+                                         ctypes.POINTER(ctypes.c_int)]),
+    "lpbf_b200_advance_launches": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.POINTER(Opts)]),
+    "lpbf_b200_read_error": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_uint)]),
+}
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def lib(build_if_needed: bool = True):
+    """Load liblpbf_b200.so, building it first if it is missing or stale."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if build_if_needed and (_build.stale() and _can_build()):
+                _build.build()
+            if not os.path.exists(_build.LIB):
+                raise RuntimeError(f"{_build.LIB} is missing and could not be built")
+            L = ctypes.CDLL(_build.LIB)
+            for name, (res, args) in SIGNATURES.items():
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+            _lib = L
+    return _lib
+
+
+def _can_build() -> bool:
+    try:
+        _build.nvcc()
+        return True
+    except RuntimeError:
+        return False
+
+
+def check(status: int, what: str = "liblpbf_b200") -> None:
+    if status != LPBF_OK:
+        msg = lib().lpbf_b200_status_string(status).decode()
+        raise RuntimeError(f"{what}: status {status} ({msg})")
+
+
+__all__ = ["lib", "lib_path", "check", "Opts", "SIGNATURES", "StepConst", "Partial", "Tick"]

@@ -1,0 +1,189 @@
+// SPDX-License-Identifier: 0BSD
+// ---------------------------------------------------------------------------
+// Device building blocks shared by every kernel of liblpbf_b200:
+//   * Coef / LaserSub: the per-launch constants, pre-scaled by dt on the host;
+//   * cell_update: the baseline explicit-Euler update of one cell;
+//   * PTX wrappers for mbarriers and TMA (cp.async.bulk.tensor) loads;
+//   * the Partial combine rule (max T, ties -> smallest flat index, min/max
+//     molten row) used by every reduction.
+//
+// The update evaluates the reference's step (include/step_task.hpp:95-129,
+// src/gpu/kernels.cu:106-124)
+//     T' = T + dt * ( alpha*(lap_x + lap_y) + S - loss(T) )
+// with every dt-scaled coefficient folded on the host:
+//     T' = T + ( ax*(R + L - 2T) + ay*(U + D - 2T) + S_dt - loss_dt(T) ).
+// Each term is kept as a difference that is exactly zero at equilibrium
+// (uniform field at the ambient temperature), so untouched far-field cells
+// stay bit-exactly at T_amb, as in the reference; all other differences are
+// rounding of the increment, far below 1e-12 of T.
+// ---------------------------------------------------------------------------
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lpbf_step_const.hpp"
+
+namespace lpbf_b200 {
+
+constexpr int KMAX = 8;            // most time steps one launch can carry
+constexpr double SIGMA_SB = 5.670374419e-8;
+// exp(x) is exactly +0 in double for x < -745.14; cells whose Gaussian
+// exponent is at or below -750 get S = 0 without evaluating exp.
+constexpr double EXP_CUT = 750.0;
+
+struct LaserSub {
+    double x_l, y_l;
+    double cs;                     // dt * q_scale * peak_S / (rho_cp * h)
+};
+
+struct Coef {
+    int    nx, ny;
+    double dx, dy;
+    double ax, ay;                 // dt*alpha/dx^2, dt*alpha/dy^2
+    double c_conv, c_sub, c_ls;    // dt*hConv/(h rho cp), dt*(K/dSub)/(h rho cp), their sum
+    double c_rad;                  // dt*eps*sigma/(h rho cp), 0 without radiation
+    double Tamb, Tsub, Tamb4;      // Tamb4 = (Tamb*Tamb)*(Tamb*Tamb)
+    double m2r;                    // -2 / r0^2
+    double r2_cut;                 // r^2 beyond which S is exactly 0
+    double Tm;                     // melt threshold of the reduction
+    double T_edge;                 // fixed edge temperature (bc == 1)
+    int    bc;                     // 0 mirror (ghost = centre), 1 fixed edges
+    int    same_T;                 // Tamb == Tsub: one conduction term
+};
+
+// Host: fold a reference StepConst into launch constants.
+inline Coef make_coef(const StepConst& k, int bc, double T_edge, double Tm) {
+    Coef c{};
+    c.nx = k.nx; c.ny = k.ny;
+    c.dx = k.dx; c.dy = k.dy;
+    c.ax = k.dt * k.alpha * k.inv_dx2;
+    c.ay = k.dt * k.alpha * k.inv_dy2;
+    const double s = k.dt * k.inv_h / k.rho_cp;
+    c.c_conv = s * k.hConv;
+    c.c_sub  = s * (k.K / k.dSub);
+    c.c_ls   = c.c_conv + c.c_sub;
+    c.c_rad  = k.radiation ? s * (k.eps * SIGMA_SB) : 0.0;
+    c.Tamb = k.Tamb; c.Tsub = k.Tsub;
+    const double ta2 = k.Tamb * k.Tamb;
+    c.Tamb4 = ta2 * ta2;
+    c.m2r = -2.0 * k.inv_r0_sq;
+    c.r2_cut = (0.5 * EXP_CUT) / k.inv_r0_sq;
+    c.Tm = Tm; c.T_edge = T_edge; c.bc = bc;
+    c.same_T = (k.Tamb == k.Tsub) ? 1 : 0;
+    return c;
+}
+
+inline LaserSub make_laser(const StepConst& k, double x_l, double y_l, double q_scale) {
+    LaserSub l;
+    l.x_l = x_l; l.y_l = y_l;
+    l.cs = k.dt * (q_scale * k.peak_S) / (k.rho_cp * k.h);
+    return l;
+}
+
+// Loss increment dt*loss(T)/... for one cell.
+__device__ __forceinline__ double loss_dt(double T, const Coef& c) {
+    const double da = T - c.Tamb;
+    const double t2 = T * T;
+    const double e4 = t2 * t2 - c.Tamb4;
+    double lin;
+    if (c.same_T) lin = c.c_ls * da;
+    else          lin = fma(c.c_sub, T - c.Tsub, c.c_conv * da);
+    return fma(c.c_rad, e4, lin);
+}
+
+// Baseline update of one interior-formula cell; S_dt already dt-scaled.
+__device__ __forceinline__ double cell_update(double T, double L, double R,
+                                              double U, double D, double S_dt,
+                                              const Coef& c) {
+    const double lx = fma(-2.0, T, R + L);
+    const double ly = fma(-2.0, T, U + D);
+    const double inc = fma(c.ax, lx, c.ay * ly);
+    return T + ((inc + S_dt) - loss_dt(T, c));
+}
+__device__ __forceinline__ double cell_update_nosrc(double T, double L, double R,
+                                                    double U, double D, const Coef& c) {
+    const double lx = fma(-2.0, T, R + L);
+    const double ly = fma(-2.0, T, U + D);
+    const double inc = fma(c.ax, lx, c.ay * ly);
+    return T + (inc - loss_dt(T, c));
+}
+
+// Gaussian source increment at column x of a row whose (y - y_l)^2 is dy2.
+__device__ __forceinline__ double source_dt(int x, double dy2, const LaserSub& l,
+                                            const Coef& c) {
+    const double dxl = __dsub_rn(__dmul_rn((double)x, c.dx), l.x_l);
+    const double r2 = __dadd_rn(__dmul_rn(dxl, dxl), dy2);
+    if (r2 >= c.r2_cut) return 0.0;
+    return l.cs * exp(__dmul_rn(c.m2r, r2));
+}
+
+// ---- Partial combine: larger T wins, equal T -> smaller index ------------
+__device__ __forceinline__ void partial_take(double& tm, long long& ag, int& mn, int& mx,
+                                             double t2, long long a2, int mn2, int mx2) {
+    if (t2 > tm || (t2 == tm && a2 < ag)) { tm = t2; ag = a2; }
+    mn = min(mn, mn2);
+    mx = max(mx, mx2);
+}
+__device__ __forceinline__ void partial_warp_reduce(double& tm, long long& ag, int& mn, int& mx) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double t2 = __shfl_xor_sync(0xffffffffu, tm, off);
+        const long long a2 = __shfl_xor_sync(0xffffffffu, ag, off);
+        const int mn2 = __shfl_xor_sync(0xffffffffu, mn, off);
+        const int mx2 = __shfl_xor_sync(0xffffffffu, mx, off);
+        partial_take(tm, ag, mn, mx, t2, a2, mn2, mx2);
+    }
+}
+
+// ---- PTX: shared-memory addresses, mbarriers, TMA ----------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Wait for an mbarrier phase with a time limit (1 s).  Returns false when the
+// limit ran out; the caller then records an error and stops issuing work.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (globaltimer_ns() - t0 > 1000000000ull) return false;
+    }
+    return true;
+}
+// 2D tiled TMA load of box (x, y) into this CTA's shared memory.  x must be
+// even for f64 (16-byte rule); y may be negative or past the end (zero fill).
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];"
+        :: "r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y),
+           "r"(smem_u32(bar))
+        : "memory");
+}
+
+}  // namespace lpbf_b200

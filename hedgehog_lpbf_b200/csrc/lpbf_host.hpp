@@ -1,0 +1,60 @@
+// SPDX-License-Identifier: 0BSD
+// ---------------------------------------------------------------------------
+// Host-side helpers shared by the translation units of liblpbf_b200.so:
+// device properties, the workspace layout, TMA tensor-map encoding (through
+// the driver entry point, so the library does not link libcuda directly) and
+// the launch functions each unit exports to the others.
+// ---------------------------------------------------------------------------
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "lpbf_device.cuh"
+
+namespace lpbf_b200 {
+
+constexpr int MAX_CTAS = 2048;     // most CTAs a reducing launch may use
+
+// Device workspace.  The counter and error word sit in the first 256 bytes;
+// per-CTA partials follow.
+struct Workspace {
+    unsigned int counter;
+    unsigned int err;
+    unsigned int pad[62];
+    Partial parts[MAX_CTAS * KMAX];
+};
+static_assert(offsetof(Workspace, parts) == 256, "workspace header");
+
+int sm_count();                    // of the current device
+
+// Encode (or fetch from a small cache) a 2D f64 tensor map over a row-major
+// nx x ny field with box {box_cols, box_rows}.  Returns false on failure.
+bool tensor_map_f64(const void* base, int nx, int ny, int box_cols, int box_rows,
+                    CUtensorMap* out);
+bool tensor_map_f32(const void* base, int nx, int ny, int box_cols, int box_rows,
+                    CUtensorMap* out);
+
+// True when `p` suits the TMA path (16-byte aligned base, even row length).
+inline bool tma_ok(const void* p, int nx) {
+    return (reinterpret_cast<uintptr_t>(p) % 16 == 0) && (nx % 2 == 0);
+}
+
+// Baseline-physics advance of `K` steps in one launch (K = 1..4).
+//   ring   : K finalized Partials (null: no reduction)
+//   ref_out: reference fused-reduce layout (K == 1 only), ref_nparts entries
+// Returns a CUDA error code.
+cudaError_t launch_advance(int K, const double* Tin, double* Tout, const Coef& c,
+                           const LaserSub* las, Partial* ring, Workspace* ws,
+                           Partial* ref_out, long long ref_nparts, int rows,
+                           cudaStream_t stream);
+
+// Extended-physics (phys == 1) single step, one thread per cell, with the
+// same reduction outputs as launch_advance.
+cudaError_t launch_ext_step(const double* Tin, double* Tout, const StepConst& k,
+                            int bc, double T_edge, double Tm, Partial* ring,
+                            Workspace* ws, Partial* ref_out, long long ref_nparts,
+                            cudaStream_t stream);
+
+}  // namespace lpbf_b200

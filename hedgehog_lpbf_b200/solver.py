@@ -1,0 +1,121 @@
+# SPDX-License-Identifier: 0BSD
+"""Python host API over the C-ABI: a device-resident field that advances
+along a laser plan.
+
+PyTorch provides device memory and streams only; every kernel runs in
+liblpbf_b200.so through ``lpbf_b200_advance``.  The per-step results are the
+reference's ``Partial`` records (peak T, argmax flat index with smallest-index
+ties, molten row extent), as produced by the reference's reduce + finalize
+(src/gpu/kernels.cu:205-262).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .params import StepConst
+from .plan import TICK_DTYPE
+
+PARTIAL_DTYPE = np.dtype({"names": ["tmax", "arg", "ymin", "ymax"],
+                          "formats": [np.float64, np.int64, np.int32, np.int32],
+                          "offsets": [0, 8, 16, 20], "itemsize": 24})
+
+
+def _stream_handle(stream: torch.cuda.Stream | None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def ring_to_numpy(ring: torch.Tensor) -> np.ndarray:
+    """Device ring (uint8 tensor) -> numpy PARTIAL_DTYPE array."""
+    return ring.cpu().numpy().view(PARTIAL_DTYPE)
+
+
+class Solver:
+    """Two device fields (ping-pong), the workspace and the metric ring of one
+    simulation.  ``advance`` runs a plan slice; ``field`` is the current field.
+
+    depth: time steps per launch (temporal blocking), 0 = automatic.
+    bc: 0 zero-flux mirror edges (the reference's), 1 fixed edges at T_edge.
+    """
+
+    def __init__(self, k: StepConst, *, phys: int = 0, bc: int = 0, T_edge: float = 300.0,
+                 Tm: float = 1609.0, depth: int = 0, rows: int = 0,
+                 device: torch.device | str | None = None, T0: float | np.ndarray | None = None):
+        self.lib = _lib.lib()
+        self.k = StepConst.from_buffer_copy(bytes(k))
+        self.nx, self.ny = k.nx, k.ny
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        self.opts = _lib.Opts(phys=phys, bc=bc, T_edge=T_edge, Tm=Tm, depth=depth, rows=rows)
+        shape = (self.ny, self.nx)
+        self.bufs = [torch.empty(shape, dtype=torch.float64, device=self.device),
+                     torch.empty(shape, dtype=torch.float64, device=self.device)]
+        self.cur = 0
+        nbytes = self.lib.lpbf_b200_workspace_bytes()
+        self.work = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.lpbf_b200_workspace_init(
+                self.work.data_ptr(), nbytes, _stream_handle(None)), "workspace_init")
+        if T0 is None:
+            T0 = k.Tamb
+        self.set_field(T0)
+
+    @property
+    def field(self) -> torch.Tensor:
+        return self.bufs[self.cur]
+
+    def set_field(self, T0) -> None:
+        if np.isscalar(T0):
+            self.bufs[self.cur].fill_(float(T0))
+        else:
+            src = torch.as_tensor(np.asarray(T0, dtype=np.float64).reshape(self.ny, self.nx))
+            self.bufs[self.cur].copy_(src)
+
+    def new_ring(self, n_steps: int) -> torch.Tensor:
+        return torch.zeros(n_steps * 24, dtype=torch.uint8, device=self.device)
+
+    def launches(self, n_steps: int) -> int:
+        return self.lib.lpbf_b200_advance_launches(self.nx, self.ny, n_steps,
+                                                   ctypes.byref(self.opts))
+
+    def advance(self, plan: np.ndarray, ring: torch.Tensor | None = None,
+                stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+        """Advance by len(plan) steps (plan: TICK_DTYPE array on the host).
+        ring: uint8 device tensor of >= 24*len(plan) bytes, or None."""
+        plan = np.ascontiguousarray(plan, dtype=TICK_DTYPE)
+        n = len(plan)
+        if ring is not None and ring.numel() < 24 * n:
+            raise ValueError("ring too small")
+        in_b = ctypes.c_int(0)
+        a = self.bufs[self.cur]
+        b = self.bufs[1 - self.cur]
+        with torch.cuda.device(self.device):
+            st = self.lib.lpbf_b200_advance(
+                a.data_ptr(), b.data_ptr(), ctypes.byref(self.k),
+                plan.ctypes.data if n else None, n, ctypes.byref(self.opts),
+                ring.data_ptr() if ring is not None else None,
+                self.work.data_ptr(), self.work.numel(), _stream_handle(stream),
+                ctypes.byref(in_b))
+        _lib.check(st, "lpbf_b200_advance")
+        if in_b.value:
+            self.cur = 1 - self.cur
+        return self.field
+
+    def read_error(self) -> int:
+        err = ctypes.c_uint(0)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.lpbf_b200_read_error(self.work.data_ptr(), _stream_handle(None),
+                                                     ctypes.byref(err)), "read_error")
+        return err.value
+
+    def run(self, T0_host: np.ndarray, plan: np.ndarray, pinned_out: np.ndarray | None = None):
+        """End-to-end call on host data: copy T0 in, advance along the plan,
+        copy the final field and the per-step Partials out."""
+        self.set_field(T0_host)
+        ring = self.new_ring(len(plan))
+        self.advance(plan, ring)
+        T = self.field.cpu().numpy()
+        return T, ring_to_numpy(ring)

@@ -1,0 +1,100 @@
+/* SPDX-License-Identifier: 0BSD
+ * ---------------------------------------------------------------------------
+ * liblpbf_b200 extended C-ABI: multi-step, status-returning entry points.
+ *
+ * Plain C (usable from C, C++, ctypes, cgo, JNI): pointers, sizes, POD
+ * structs whose layouts equal the reference's StepConst / Partial / Tick.
+ * Every entry point is asynchronous on `stream` unless noted, allocates
+ * nothing, and returns LPBF_OK (0) or a negative status (lpbf_b200_status_string).
+ *
+ * Reference interfaces these replace or extend:
+ *   lpbf_b200_advance   the per-step loop of GpuStepTask::execute
+ *                       (include/gpu_step_task.hpp:149-197): step + reduce +
+ *                       finalize for `n_steps` Ticks of a plan, in
+ *                       ceil(n_steps / depth) launches instead of 2-4
+ *                       launches per step.
+ * ---------------------------------------------------------------------------
+ */
+#ifndef LPBF_B200_H
+#define LPBF_B200_H
+
+#include <stddef.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+#include "lpbf_step_const.hpp"
+#include "gpu_messages.hpp"
+typedef lpbf::Tick lpbf_tick;
+extern "C" {
+#else
+#include <stdbool.h>
+typedef struct StepConst {
+    int nx, ny;
+    double dx, dy, inv_dx2, inv_dy2, inv_r0_sq;
+    double alpha, K, rho, cp, rho_cp, inv_h, h, dt;
+    double peak_S, eta, P;
+    double hConv, Tamb, Tsub, dSub, eps;
+    bool radiation;
+    double kmult;
+    double x_l, y_l;
+    double q_scale;
+} StepConst;
+typedef struct Partial { double tmax; long long arg; int ymin; int ymax; } Partial;
+typedef struct lpbf_tick {
+    int step; double t; double x_l, y_l; double q_scale; double x_laser_csv;
+    bool wrapped; bool dump;
+} lpbf_tick;
+#endif
+
+enum {
+    LPBF_OK = 0,
+    LPBF_ERR_ARG = -1,          /* invalid argument */
+    LPBF_ERR_UNSUPPORTED = -2,  /* valid request this build does not implement */
+    LPBF_ERR_WORKSPACE = -3,    /* workspace missing or too small */
+    LPBF_ERR_CUDA = -4,         /* a CUDA runtime call or launch failed */
+    LPBF_ERR_TMA = -5           /* tensor-map encoding failed */
+};
+
+/* Options of a multi-step advance. */
+typedef struct lpbf_b200_opts {
+    int    phys;     /* 0 constant properties (baseline); 1 extended (Mills k(T), cp(T)) */
+    int    bc;       /* 0 zero-flux mirror edges (the reference's); 1 fixed-value edges */
+    double T_edge;   /* edge temperature for bc == 1 [K] */
+    double Tm;       /* melt threshold of the per-step Partial [K] */
+    int    depth;    /* time steps per launch (temporal blocking, 1..4); 0 = automatic */
+    int    rows;     /* rows per warp task; 0 = automatic */
+} lpbf_b200_opts;
+
+int         lpbf_b200_version(void);
+const char* lpbf_b200_status_string(int status);
+
+/* Device workspace (per-launch partials, a ticket counter and an error word).
+ * Size is independent of the grid.  Zero it once with
+ * lpbf_b200_workspace_init before its first use; advance leaves it ready for
+ * the next call.  Calls that share one workspace must be stream-ordered. */
+size_t lpbf_b200_workspace_bytes(void);
+int    lpbf_b200_workspace_init(void* work, size_t work_bytes, cudaStream_t stream);
+
+/* Advance the field by n_steps time steps along plan[0..n_steps) (host array;
+ * each step uses plan[i].x_l, y_l, q_scale and k->dt).  The field starts in
+ * T_a; T_a and T_b are a ping-pong pair of nx*ny doubles (row-major, must not
+ * overlap).  On return *result_in_b tells which buffer holds the final field
+ * (this is known on the host at once: the launch count's parity).  ring
+ * (device, nullable) receives one finalized Partial per step, ring[i] for
+ * step i.  Capturable in a CUDA graph (no host synchronization). */
+int lpbf_b200_advance(double* T_a, double* T_b, const StepConst* k,
+                      const lpbf_tick* plan, int n_steps, const lpbf_b200_opts* opts,
+                      Partial* ring, void* work, size_t work_bytes,
+                      cudaStream_t stream, int* result_in_b);
+
+/* Number of launches lpbf_b200_advance issues for these arguments. */
+int lpbf_b200_advance_launches(int nx, int ny, int n_steps, const lpbf_b200_opts* opts);
+
+/* Copy the workspace error word to *err (synchronizes `stream`); bit 0 means
+ * a TMA wait exceeded its time limit and the launch stopped early. */
+int lpbf_b200_read_error(const void* work, cudaStream_t stream, unsigned int* err);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+#endif /* LPBF_B200_H */

@@ -1,0 +1,68 @@
+# SPDX-License-Identifier: 0BSD
+"""The C-ABI library loads and exports every symbol include/*.h declares, and
+the headers compile from C and C++ and link against it.  No GPU needed: no
+compute entry point is called."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from hedgehog_lpbf_b200 import _lib, build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INC = os.path.join(ROOT, "include")
+DECL = re.compile(r"^\s*(?:void|int|size_t|const\s+char\s*\*)\s*\**\s*(lpbf_\w+)\s*\(", re.M)
+
+
+def declared_symbols():
+    names = set()
+    for f in os.listdir(INC):
+        if f.endswith((".h", ".hpp")):
+            names |= set(DECL.findall(open(os.path.join(INC, f)).read()))
+    return sorted(names)
+
+
+def test_every_declared_symbol_is_bound_and_exported():
+    names = declared_symbols()
+    assert "lpbf_launch_step" in names and "lpbf_b200_advance" in names
+    L = _lib.lib()
+    for n in names:
+        assert n in _lib.SIGNATURES, f"{n} declared in include/ but not bound in _lib"
+        assert hasattr(L, n), f"{n} not exported by {build.LIB}"
+    assert set(_lib.SIGNATURES) == set(names)
+
+
+def test_host_only_entry_points():
+    L = _lib.lib()
+    assert L.lpbf_b200_version() >= 1
+    assert L.lpbf_b200_workspace_bytes() >= 256
+    assert L.lpbf_b200_status_string(0) == b"ok"
+    o = _lib.Opts(phys=0, bc=0, T_edge=300.0, Tm=1609.0, depth=4, rows=0)
+    assert L.lpbf_b200_advance_launches(512, 512, 10, ctypes.byref(o)) == 3
+    # argument validation happens before any CUDA call
+    assert L.lpbf_b200_advance(None, None, None, None, 0, None, None, None, 0, None, None) == -1
+
+
+@pytest.mark.parametrize("lang", ["c", "c++"])
+def test_headers_compile_and_link(tmp_path, lang):
+    src = tmp_path / ("t.c" if lang == "c" else "t.cpp")
+    if lang == "c":
+        src.write_text('#include "lpbf_b200.h"\n#include <stdio.h>\n'
+                       'int main(void){ printf("%d %zu\\n", lpbf_b200_version(),'
+                       ' sizeof(StepConst)); return sizeof(StepConst) != 216; }\n')
+        cc = ["gcc", "-std=c11"]
+    else:
+        src.write_text('#include "lpbf_kernels.hpp"\n#include "lpbf_b200.h"\n#include <cstdio>\n'
+                       'int main(){ void (*f)(const double*, double*, const StepConst*, int,'
+                       ' cudaStream_t) = lpbf_launch_step; (void)f;'
+                       ' std::printf("%d\\n", lpbf_b200_version()); return 0; }\n')
+        cc = ["g++", "-std=c++17"]
+    exe = tmp_path / "t"
+    libdir = os.path.dirname(build.LIB)
+    subprocess.run(cc + [str(src), "-I" + INC, "-I/usr/local/cuda/include", "-o", str(exe),
+                         "-L" + libdir, "-llpbf_b200", "-Wl,-rpath," + libdir],
+                   check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    assert out.split()[0] == "1"
