@@ -36,9 +36,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N_SIDE = 8192
+N_SIDE = 8192                  # grid side (--side for a smaller profiling case)
 N_STEPS_TOTAL = 20000
-STEPS_PER_ITER = 1000
+STEPS_PER_ITER = 1000          # time steps per bench step (--iter-steps)
 BYTES_PER_UPDATE = 16          # read T (8 B) + write T (8 B) per cell-update
 
 
@@ -313,7 +313,13 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=15.0,
                     help="seconds of CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--side", type=int, default=N_SIDE,
+                    help="grid side (smaller sides are for profiling only)")
+    ap.add_argument("--iter-steps", type=int, default=STEPS_PER_ITER,
+                    help="time steps per bench step")
     args = ap.parse_args()
+    globals()["N_SIDE"] = args.side
+    globals()["STEPS_PER_ITER"] = args.iter_steps
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

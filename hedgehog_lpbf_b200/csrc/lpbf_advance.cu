@@ -4,6 +4,7 @@
 // entry points of include/lpbf_b200.h.
 // ---------------------------------------------------------------------------
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 
@@ -102,13 +103,36 @@ bool tensor_map_f32(const void* base, int nx, int ny, int box_cols, int box_rows
 // ---- launch of one temporally blocked step ---------------------------------
 namespace {
 
+// Rows whose source term can be non-zero in any of the K substeps (a
+// superset: the kernel decides exactly, this only routes rows to the general
+// body).  Empty when every substep has the beam off.
+void laser_band(const Coef& c, const LaserSub* las, int K, int* lo, int* hi, int* xlo,
+                int* xhi) {
+    int blo = 1 << 30, bhi = -(1 << 30), cxlo = 1 << 30, cxhi = -(1 << 30);
+    const double R = std::sqrt(c.r2_cut);
+    for (int t = 0; t < K; ++t) {
+        if (las[t].cs == 0.0) continue;
+        const double y = las[t].y_l, x = las[t].x_l;
+        if (!std::isfinite(y) || !std::isfinite(x) || !std::isfinite(R) || c.dy <= 0.0 ||
+            c.dx <= 0.0) {
+            blo = -2; bhi = c.ny + 2; cxlo = -2; cxhi = c.nx + 2;
+            break;
+        }
+        auto clampi = [](double v, double a, double b) { return (int)std::max(a, std::min(v, b)); };
+        blo = std::min(blo, clampi(std::floor((y - R) / c.dy) - 2.0, -2.0, c.ny + 2.0));
+        bhi = std::max(bhi, clampi(std::ceil((y + R) / c.dy) + 2.0, -2.0, c.ny + 2.0));
+        cxlo = std::min(cxlo, clampi(std::floor((x - R) / c.dx) - 2.0, -2.0, c.nx + 2.0));
+        cxhi = std::max(cxhi, clampi(std::ceil((x + R) / c.dx) + 2.0, -2.0, c.nx + 2.0));
+    }
+    *lo = blo; *hi = bhi; *xlo = cxlo; *xhi = cxhi;
+}
+
 template <int K, bool TMA, bool REDUCE>
 cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const LaserSub* las,
                      Partial* ring, Workspace* ws, Partial* ref_out, long long ref_nparts,
                      int rows, cudaStream_t stream) {
-    using G = AdvGeo<K>;
     auto kern = advance_kernel<K, TMA, REDUCE>;
-    const size_t smem = TMA ? G::SMEM_BYTES : 0;
+    const size_t smem = TMA ? ADV_SMEM_BYTES : 0;
 
     static int occ[64] = {0};
     int dev = 0;
@@ -132,11 +156,19 @@ cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const Laser
     std::memset(&p, 0, sizeof(p));
     p.c = c;
     for (int t = 0; t < K; ++t) p.las[t] = las[t];
-    p.nstrips = (c.nx + G::WOUT - 1) / G::WOUT;
+    laser_band(c, las, K, &p.band_lo, &p.band_hi, &p.bandx_lo, &p.bandx_hi);
+    p.nstrips = (c.nx + ADV_WOUT - 1) / ADV_WOUT;
+    // Dynamic scheduling (workspace given): short chunks, many tasks per
+    // warp.  Static: about one task per resident warp.
+    const bool dynamic = ws != nullptr;
     int H = rows;
     if (H <= 0) {
-        const int want = std::max(1, (resident * ADV_WARPS) / p.nstrips);
-        H = (c.ny + want - 1) / want;
+        if (dynamic) {
+            H = 32;
+        } else {
+            const int want = std::max(1, (resident * ADV_WARPS) / p.nstrips);
+            H = (c.ny + want - 1) / want;
+        }
         H = std::max(H, std::max(8, 4 * K));
     }
     p.H = std::min(H, c.ny);
@@ -151,14 +183,16 @@ cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const Laser
     p.ring = ring;
     p.ref_out = ref_out;
     p.ref_nparts = ref_nparts;
+    p.st256 = (c.nx % 4 == 0) && (reinterpret_cast<uintptr_t>(Tout) % 32 == 0);
     if (ws) {
         p.scratch = ws->parts;
         p.counter = &ws->counter;
+        p.tasks = &ws->tasks;
         p.err = &ws->err;
     }
     CUtensorMap map;
     std::memset(&map, 0, sizeof(map));
-    if (TMA && !tensor_map_f64(Tin, c.nx, c.ny, G::COLS, ADV_R, &map))
+    if (TMA && !tensor_map_f64(Tin, c.nx, c.ny, ADV_COLS, ADV_R, &map))
         return cudaErrorNotSupported;
     kern<<<grid, ADV_WARPS * 32, smem, stream>>>(map, p);
     return cudaGetLastError();

@@ -3,104 +3,202 @@
 // The temporally blocked step kernel.
 //
 // Work decomposition.  The nx x ny field (row-major f64) is cut into column
-// strips of WOUT owned columns and row chunks of H owned rows; one warp owns
-// one (strip, chunk) task at a time.  A warp covers COLS = 64*NCH columns,
-// i.e. its owned columns plus KH (= K rounded up to even) halo columns on each
-// side, so it can advance its strip K time steps with no data from other
-// warps: after level t the outermost t halo columns are stale, after K levels
-// exactly the owned columns remain valid.
+// strips of WOUT = 120 owned columns and row chunks of H owned rows; a warp
+// advances one (strip, chunk) task at a time by K time steps.  A warp covers
+// COLS = 128 columns: its owned columns plus KH = 4 halo columns per side, so
+// it needs no data from other warps (after level t the outermost t halo
+// columns are stale; after K <= 4 levels the owned columns are still exact).
+// Warps take tasks from an atomic counter (balanced: the laser rows cost
+// more) when a workspace is given, round-robin otherwise.
 //
-// Lane layout.  Lane l holds columns 64q + 2l + {0,1} of chunk q, so every
-// row access is a conflict-free 512-byte vector access per chunk, and the x
-// neighbours come from the adjacent lane by one warp shuffle each.
+// Lane layout.  Lane l holds the four consecutive columns 4l..4l+3 of the
+// strip: lanes 1..30 own all their cells, lanes 0 and 31 are halo.  The x
+// neighbours of a lane's first and last cell come from the adjacent lanes by
+// one warp shuffle each.
 //
-// Wavefront.  Rows stream top to bottom.  Level-0 rows arrive through a
-// per-warp TMA pipeline (S stages of R rows, one mbarrier per stage, no CTA
-// barrier anywhere in the stream).  At iteration j the warp loads level-0 row
-// j and computes level-t row j-t for t = 1..K, each from the three rows of
-// level t-1 held in registers.  Level-t row r lives in register slot r % 3;
-// the row loop is unrolled by three so every slot index is a compile-time
-// constant and no register is ever moved.  Level K rows are written straight
-// to HBM as 16-byte stores.
+// Wavefront.  Rows stream top to bottom in boxes of three rows, each box one
+// TMA load into a per-warp stage ring (S stages, one mbarrier per stage, no
+// CTA barrier anywhere in the stream).  At iteration j the warp takes level-0
+// row j from the stage and computes level-t row j-t for t = 1..K from the
+// three rows of level t-1 held in registers.  Level-t row r lives in register
+// slot r % 3; a box is exactly one turn of the slot rotation, so every slot
+// index is a compile-time constant and no register is moved.  Level-K rows
+// go straight to HBM as 32-byte stores.
+//
+// Fast and general boxes.  A box whose rows, over all K levels, are interior
+// to the domain, carry no source and lie in a strip away from the x edges
+// runs a branch-free body; rows of the chunk's own halo are computed there
+// too and only masked out of the store and the reduction (a value outside a
+// level's valid range only ever feeds rows that are themselves outside the
+// next level's range).  Every other box runs the general body, which handles
+// domain edges, fixed-value boundaries, partial ownership and the Gaussian
+// source (evaluated out of line, so exp is not replicated).  Both bodies evaluate
+// every cell with the same function, so results depend neither on the body
+// nor on K, H or the task order.
 //
 // Reduction.  For every level (= time step) each lane keeps the peak T with
-// its flat index and the molten row extent over its owned cells; warps,
-// then CTAs combine them, and the last CTA to finish (atomic ticket, no
-// waiting) reduces the per-CTA partials into one Partial per time step.
+// its flat index, and each warp the molten row extent (warp vote), over owned
+// cells; warps, then CTAs combine them, and the last CTA to finish (atomic
+// ticket, no waiting) reduces the per-CTA partials into one Partial per step
+// and re-arms the counters for the next launch.
 // ---------------------------------------------------------------------------
 #pragma once
+#include <stddef.h>
+
 #include "lpbf_device.cuh"
 
 namespace lpbf_b200 {
 
 constexpr int ADV_WARPS = 4;       // warps per CTA
-constexpr int ADV_NCH = 2;         // 64-column chunks per warp (COLS = 128)
-constexpr int ADV_R = 4;           // rows per TMA box
+constexpr int ADV_COLS = 128;      // columns per warp strip
+constexpr int ADV_KH = 4;          // halo columns per side (supports K <= 4)
+constexpr int ADV_WOUT = ADV_COLS - 2 * ADV_KH;
+constexpr int ADV_V = 4;           // values per lane per row
+constexpr int ADV_R = 3;           // rows per TMA box (= the register slot rotation)
 constexpr int ADV_S = 4;           // TMA stages per warp
-
-template <int K>
-struct AdvGeo {
-    static constexpr int KH = (K + 1) & ~1;
-    static constexpr int COLS = 64 * ADV_NCH;
-    static constexpr int WOUT = COLS - 2 * KH;
-    static constexpr int V = 2 * ADV_NCH;
-    static constexpr int STAGE_DOUBLES = ADV_R * COLS;
-    static constexpr size_t SMEM_BYTES =
-        size_t(ADV_WARPS) * ADV_S * STAGE_DOUBLES * sizeof(double)
-        + size_t(ADV_WARPS) * ADV_S * sizeof(uint64_t);
-};
+constexpr int ADV_STAGE_DOUBLES = ADV_R * ADV_COLS;
+constexpr size_t ADV_SMEM_BYTES =
+    size_t(ADV_WARPS) * ADV_S * ADV_STAGE_DOUBLES * sizeof(double)
+    + size_t(ADV_WARPS) * ADV_S * sizeof(uint64_t);
 
 struct AdvParams {
     Coef c;
     LaserSub las[KMAX];
+    int band_lo, band_hi;          // rows any substep's source can reach (union)
+    int bandx_lo, bandx_hi;        // columns any substep's source can reach (union)
     int nstrips, nchunks, H, ntasks;
     const double* Tin;             // source field (used by the direct-load path)
     double* Tout;                  // destination field (never aliases Tin)
     Partial* ring;                 // K finalized Partials (one per step), or null
     Partial* scratch;              // per-CTA partials, gridDim.x * K entries
     unsigned int* counter;         // last-CTA ticket, zero between launches
+    unsigned int* tasks;           // task counter (dynamic scheduling), or null
     unsigned int* err;             // error word (bit 0: TMA wait timed out)
     Partial* ref_out;              // reference fused-reduce layout (K == 1), or null
     long long ref_nparts;          // number of entries of ref_out to define
+    int st256;                     // 32-byte aligned rows: 256-bit stores
 };
 
 __host__ __device__ constexpr int mod3(int a) { return ((a % 3) + 3) % 3; }
 
-// One warp advancing one task (strip, chunk) by K levels.
+// Hot coefficients, held in registers for the whole kernel.
+struct HotCoef {
+    double ax, ay, cls, crad, Ta, Ta4;
+};
+
+// The update of one cell from its four neighbours (Tamb == Tsub form).  The
+// multiplies and fused multiply-adds are spelled out so that the compiler
+// cannot contract differently in different call sites: every path computes a
+// cell bit-identically.  Every term vanishes exactly for a uniform field at
+// Tamb.
+__device__ __forceinline__ double cell_inc(double T, double L, double R, double U, double D,
+                                           const HotCoef& h, double& loss) {
+    const double lx = fma(-2.0, T, R + L);
+    const double ly = fma(-2.0, T, U + D);
+    const double t2 = __dmul_rn(T, T);
+    const double e4 = __dsub_rn(__dmul_rn(t2, t2), h.Ta4);
+    loss = fma(h.crad, e4, __dmul_rn(h.cls, __dsub_rn(T, h.Ta)));
+    return fma(h.ax, lx, __dmul_rn(h.ay, ly));
+}
+__device__ __forceinline__ double cell_core(double T, double L, double R, double U, double D,
+                                            const HotCoef& h) {
+    double loss;
+    const double inc = cell_inc(T, L, R, U, D, h, loss);
+    return __dadd_rn(T, __dsub_rn(inc, loss));
+}
+__device__ __forceinline__ double cell_core_src(double T, double L, double R, double U, double D,
+                                                double S, const HotCoef& h) {
+    double loss;
+    const double inc = cell_inc(T, L, R, U, D, h, loss);
+    return __dadd_rn(T, __dsub_rn(__dadd_rn(inc, S), loss));
+}
+
+// Gaussian source increment of a lane's four cells starting at column x0
+// (out of line: the exp code exists once in the binary).
+__device__ __noinline__ double4 source4(int x0, double dy2, double x_l, double cs, double dx,
+                                        double m2r, double r2_cut) {
+    double S[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const double xd = __dsub_rn(__dmul_rn((double)(x0 + v), dx), x_l);
+        const double r2 = __dadd_rn(__dmul_rn(xd, xd), dy2);
+        S[v] = (r2 < r2_cut) ? cs * exp(__dmul_rn(m2r, r2)) : 0.0;
+    }
+    return make_double4(S[0], S[1], S[2], S[3]);
+}
+
+__device__ __forceinline__ void st_global_v4(double* p, double a, double b, double c, double d) {
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};"
+                 :: "l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+}
+// 32-byte store issued under a predicate (no branch).
+__device__ __forceinline__ void st_global_v4_pred(double* p, const double* v, bool pred) {
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %5, 0;\n\t"
+                 "@q st.global.v4.f64 [%0], {%1, %2, %3, %4};\n\t}"
+                 :: "l"(p), "d"(v[0]), "d"(v[1]), "d"(v[2]), "d"(v[3]), "r"((int)pred)
+                 : "memory");
+}
+
+// Per-warp reduction state in shared memory: lane peaks and their flat
+// indices per level, the molten row extent per level, and a staging area for
+// one level's three box rows.
+template <int K>
+struct alignas(16) RedSmem {
+    double tmx[K][32];
+    long long arg[K][32];
+    int ymn[K], ymx[K];
+    alignas(16) double box[3][32][ADV_V];   // written as 16-byte vectors
+};
+static_assert(offsetof(RedSmem<1>, box) % 16 == 0 && sizeof(RedSmem<1>) % 16 == 0, "align");
+static_assert(offsetof(RedSmem<3>, box) % 16 == 0 && sizeof(RedSmem<3>) % 16 == 0, "align");
+
 template <int K, bool TMA, bool REDUCE>
 struct WarpStrip {
-    using G = AdvGeo<K>;
-    static constexpr int V = G::V;
+    static constexpr int V = ADV_V;
 
     const AdvParams& p;
     const CUtensorMap* map;
     double* stages;                // this warp's S stages
     uint64_t* bars;                // this warp's S mbarriers
-    uint32_t& gbox;                // running box counter of this warp (phase tracking)
+    uint32_t gbox;                 // running box counter (mbarrier phase tracking)
     const int lane;
+    const HotCoef h;
 
-    int x0, xs, y0, y1, jy0, jend, nbox, issued;
-    bool edge, failed;
-    bool own[V];                   // lane's column is owned and inside the grid
+    int x0, xs, xl, y0, y1, jy0, jend, nbox, issued;
+    bool edge, failed, own_all, src_strip;
 
-    double w[K > 1 ? K : 1][3][V]; // level windows 0..K-1 (slot = row % 3)
-    double tmx[K];
-    long long targ[K];
-    int ymn[K], ymx[K];
+    double w0[3][V];                     // level-0 window (slot = row % 3)
+    double w[K > 1 ? K - 1 : 1][3][V];   // windows of levels 1..K-1
+    // Reduction state per level: the lane's resolved peak, this box's peak
+    // (resolved once per box, so no row carries a branch), the warp's molten
+    // row extent, and in shared memory the flat index of the lane's peak.
+    double thr[K];                       // per-box trigger: min(peak, Tm), +inf off-strip
+    bool hit[K];                         // a cell of this box crossed thr
+    RedSmem<K>* rs;                      // this warp's reduction state (shared memory)
 
-    __device__ WarpStrip(const AdvParams& p_, const CUtensorMap* m, double* st,
-                         uint64_t* b, uint32_t& g, int ln)
-        : p(p_), map(m), stages(st), bars(b), gbox(g), lane(ln), failed(false) {
+    __device__ __forceinline__ WarpStrip(const AdvParams& p_, const CUtensorMap* m,
+                                         double* st, uint64_t* b, int ln, RedSmem<K>* rs_)
+        : p(p_), map(m), stages(st), bars(b), gbox(0), lane(ln),
+          h{p_.c.ax, p_.c.ay, p_.c.c_ls, p_.c.c_rad, p_.c.Tamb, p_.c.Tamb4},
+          failed(false), rs(rs_) {
         const long long N = (long long)p.c.nx * p.c.ny;
+        if constexpr (REDUCE) {
 #pragma unroll
-        for (int t = 0; t < K; ++t) { tmx[t] = -1.0; targ[t] = N; ymn[t] = p.c.ny; ymx[t] = -1; }
+            for (int t = 0; t < K; ++t) {
+                hit[t] = false;
+                rs->tmx[t][lane] = -1.0;
+                rs->arg[t][lane] = N;
+                if (lane == 0) { rs->ymn[t] = p.c.ny; rs->ymx[t] = -1; }
+            }
+        }
+        __syncwarp();
     }
 
     __device__ __forceinline__ void issue(int b) {
         const uint32_t g = gbox + b;
         const int st = g % ADV_S;
-        double* dst = stages + st * G::STAGE_DOUBLES;
-        mbar_expect_tx(&bars[st], G::STAGE_DOUBLES * sizeof(double));
+        double* dst = stages + st * ADV_STAGE_DOUBLES;
+        mbar_expect_tx(&bars[st], ADV_STAGE_DOUBLES * sizeof(double));
         tma_load_2d(dst, map, xs, jy0 + b * ADV_R, &bars[st]);
         issued = b + 1;
     }
@@ -108,20 +206,18 @@ struct WarpStrip {
     __device__ __forceinline__ void run_task(int task) {
         const int nx = p.c.nx, ny = p.c.ny;
         const int strip = task % p.nstrips, chunk = task / p.nstrips;
-        x0 = strip * G::WOUT;
-        xs = x0 - G::KH;
+        x0 = strip * ADV_WOUT;
+        xs = x0 - ADV_KH;
+        xl = xs + 4 * lane;
         y0 = chunk * p.H;
         y1 = min(y0 + p.H, ny);
         jy0 = max(y0 - K, 0);
         jy0 -= jy0 % 3;
         jend = min(y1 + K, ny);
         nbox = (jend - jy0 + ADV_R - 1) / ADV_R;
-        edge = (xs <= 0) || (xs + G::COLS > nx - 1);
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-            const int x = xs + 64 * (v >> 1) + 2 * lane + (v & 1);
-            own[v] = (x >= x0) && (x < x0 + G::WOUT) && (x < nx);
-        }
+        edge = (xs <= 0) || (xs + ADV_COLS > nx - 1);
+        own_all = lane >= 1 && lane <= 30;
+        src_strip = !(xs + ADV_COLS <= p.bandx_lo || xs > p.bandx_hi);
         issued = 0;
         if constexpr (TMA) {
             if (lane == 0) {
@@ -130,10 +226,36 @@ struct WarpStrip {
             }
         }
         const int jlast = y1 - 1 + K;
-        for (int j = jy0; j <= jlast && !failed; j += 3) {
-            row<0>(j);
-            if (j + 1 <= jlast) row<1>(j + 1);
-            if (j + 2 <= jlast) row<2>(j + 2);
+        for (int b = 0, j = jy0; j <= jlast && !failed; ++b, j += ADV_R) {
+            const double* st = nullptr;
+            if (j < jend) {
+                st = wait_box(b);
+                if (failed) break;
+            }
+            // computed rows of this box: j-K .. j+1 over all levels
+            if constexpr (REDUCE) set_thresholds();
+            const bool fast = !edge && j - K >= 1 && j + 1 <= ny - 2 && p.st256 &&
+                              (!src_strip || j + 1 < p.band_lo || j - K > p.band_hi);
+            if (fast && j < jend) {
+                fast_row<0>(j, st);
+                fast_row<1>(j + 1, st);
+                fast_row<2>(j + 2, st);
+            } else {
+                general_row<0>(j, st, jlast);
+                general_row<1>(j + 1, st, jlast);
+                general_row<2>(j + 2, st, jlast);
+            }
+            if constexpr (REDUCE) resolve_box(j);
+            if constexpr (TMA) {
+                if (j < jend) {
+                    __syncwarp();
+                    if (lane == 0 && b + ADV_S < nbox) {
+                        // order this warp's reads of the stage before the refill
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        issue(b + ADV_S);
+                    }
+                }
+            }
         }
         if constexpr (TMA) {
             if (failed) drain();
@@ -151,60 +273,103 @@ struct WarpStrip {
         }
     }
 
-    __device__ __forceinline__ void load_row0(int jj, double* dst) {
-        const int nx = p.c.nx;
+    // Wait for box b; returns its stage (TMA) or null (direct loads).
+    __device__ __forceinline__ const double* wait_box(int b) {
         if constexpr (TMA) {
-            const int rel = jj - jy0;
-            const int b = rel / ADV_R, rr = rel % ADV_R;
             const uint32_t g = gbox + b;
             const int st = g % ADV_S;
-            if (rr == 0) {
-                const bool ok = mbar_wait_bounded(&bars[st], (g / ADV_S) & 1);
-                if (!__all_sync(0xffffffffu, ok)) {
-                    if (lane == 0) atomicOr(p.err, 1u);
-                    failed = true;
-                    return;
-                }
+            const bool ok = mbar_wait_bounded(&bars[st], (g / ADV_S) & 1);
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) atomicOr(p.err, 1u);
+                failed = true;
+                return nullptr;
             }
-            const double* src = stages + st * G::STAGE_DOUBLES + rr * G::COLS;
-#pragma unroll
-            for (int q = 0; q < ADV_NCH; ++q) {
-                const double2 v = *reinterpret_cast<const double2*>(src + 64 * q + 2 * lane);
-                dst[2 * q] = v.x;
-                dst[2 * q + 1] = v.y;
-            }
-            if (rr == ADV_R - 1 || jj == jend - 1) {
-                __syncwarp();
-                if (lane == 0 && b + ADV_S < nbox) {
-                    // order this warp's reads of the stage before the refill
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    issue(b + ADV_S);
-                }
-            }
+            return stages + st * ADV_STAGE_DOUBLES;
         } else {
+            return nullptr;
+        }
+    }
+
+    // Level-0 row jj (row P of the current box) into dst.
+    template <int P>
+    __device__ __forceinline__ void load_row0(int jj, const double* st, double* dst) {
+        if constexpr (TMA) {
+            const double* src = st + P * ADV_COLS + 4 * lane;
+            const double2 a = *reinterpret_cast<const double2*>(src);
+            const double2 b2 = *reinterpret_cast<const double2*>(src + 2);
+            dst[0] = a.x; dst[1] = a.y; dst[2] = b2.x; dst[3] = b2.y;
+        } else {
+            const int nx = p.c.nx;
             const double* rowp = p.Tin + (size_t)jj * nx;
 #pragma unroll
-            for (int q = 0; q < ADV_NCH; ++q) {
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const int x = xs + 64 * q + 2 * lane + e;
-                    dst[2 * q + e] = (x >= 0 && x < nx) ? __ldg(rowp + x) : 0.0;
-                }
+            for (int v = 0; v < V; ++v) {
+                const int x = xl + v;
+                dst[v] = (x >= 0 && x < nx) ? __ldg(rowp + x) : 0.0;
             }
         }
     }
 
+    // Window of level t (t = 0..K-1).
+    template <int T>
+    __device__ __forceinline__ double (&win())[3][V] {
+        if constexpr (T == 0) return w0;
+        else return w[T - 1];
+    }
+
+    // x neighbours of the lane's first and last cell.
+    __device__ __forceinline__ void neighbours(const double* ce, double& Lo, double& Ro) {
+        Lo = __shfl_up_sync(0xffffffffu, ce[V - 1], 1);
+        Ro = __shfl_down_sync(0xffffffffu, ce[0], 1);
+    }
+
+    // ---- fast body -------------------------------------------------------
     template <int P>
-    __device__ __forceinline__ void row(int jj) {
-        if (jj < jend) {
-            load_row0(jj, w[0][P]);
-            if (failed) return;
-        }
-        level<P, 1>(jj);
+    __device__ __forceinline__ void fast_row(int jj, const double* st) {
+        load_row0<P>(jj, st, win<0>()[P]);
+        fast_level<P, 1>(jj);
     }
 
     template <int P, int T>
-    __device__ __forceinline__ void level(int jj) {
+    __device__ __forceinline__ void fast_level(int jj) {
+        if constexpr (T <= K) {
+            constexpr int su = mod3(P - T - 1), sc = mod3(P - T), sd = mod3(P - T + 1);
+            double (&wn)[3][V] = win<T - 1>();
+            const double* up = wn[su];
+            const double* ce = wn[sc];
+            const double* dn = wn[sd];
+            double Lo, Ro;
+            neighbours(ce, Lo, Ro);
+            double nv[V];
+            nv[0] = cell_core(ce[0], Lo, ce[1], up[0], dn[0], h);
+            nv[1] = cell_core(ce[1], ce[0], ce[2], up[1], dn[1], h);
+            nv[2] = cell_core(ce[2], ce[1], ce[3], up[2], dn[2], h);
+            nv[3] = cell_core(ce[3], ce[2], Ro, up[3], dn[3], h);
+            const int r = jj - T;
+            // Rows outside [y0, y1) are this chunk's halo: computed (their
+            // values only ever feed other halo rows) but not stored or reduced.
+            const bool owned_row = r >= y0 && r < y1;
+            if constexpr (T < K) {
+                double (&wo)[3][V] = win<T>();
+#pragma unroll
+                for (int v = 0; v < V; ++v) wo[sc][v] = nv[v];
+            } else {
+                st_global_v4_pred(p.Tout + (size_t)r * p.c.nx + xl, nv, owned_row && own_all);
+            }
+            if constexpr (REDUCE) row_stats<T - 1>(r, nv, own_all && owned_row, true);
+            fast_level<P, T + 1>(jj);
+        }
+    }
+
+    // ---- general body ----------------------------------------------------
+    template <int P>
+    __device__ __forceinline__ void general_row(int jj, const double* st, int jlast) {
+        if (jj > jlast) return;
+        if (jj < jend) load_row0<P>(jj, st, win<0>()[P]);
+        general_level<P, 1>(jj);
+    }
+
+    template <int P, int T>
+    __device__ __forceinline__ void general_level(int jj) {
         if constexpr (T <= K) {
             constexpr int su = mod3(P - T - 1), sc = mod3(P - T), sd = mod3(P - T + 1);
             const int ny = p.c.ny;
@@ -212,37 +377,41 @@ struct WarpStrip {
             const int lo = max(y0 - K + T, 0);
             const int hi = min(y1 - 1 + K - T, ny - 1);
             if (r >= lo && r <= hi) {
-                double (&win)[3][V] = w[T - 1];
+                double (&wn)[3][V] = win<T - 1>();
                 // Mirror edges: the ghost row is the centre row.  The slot of
                 // row -1 (row 2) is not filled yet and the slot of row ny
                 // (row ny-3) is no longer needed, so both can be overwritten.
                 if (r == 0) {
 #pragma unroll
-                    for (int v = 0; v < V; ++v) win[su][v] = win[sc][v];
+                    for (int v = 0; v < V; ++v) wn[su][v] = wn[sc][v];
                 }
                 if (r == ny - 1) {
 #pragma unroll
-                    for (int v = 0; v < V; ++v) win[sd][v] = win[sc][v];
+                    for (int v = 0; v < V; ++v) wn[sd][v] = wn[sc][v];
                 }
                 double nv[V];
-                compute_row(win[su], win[sc], win[sd], r, p.las[T - 1], nv);
+                compute_row_general(wn[su], wn[sc], wn[sd], r, p.las[T - 1], nv);
+                const bool owned_row = r >= y0 && r < y1;
                 if constexpr (T < K) {
+                    double (&wo)[3][V] = win<T>();
 #pragma unroll
-                    for (int v = 0; v < V; ++v) w[T][sc][v] = nv[v];
+                    for (int v = 0; v < V; ++v) wo[sc][v] = nv[v];
                 } else {
-                    if (r >= y0 && r < y1) store_row(r, nv);
+                    if (owned_row) store_row(r, nv);
                 }
-                if constexpr (REDUCE) {
-                    if (r >= y0 && r < y1) reduce_row<T - 1>(r, nv);
-                }
+                if constexpr (REDUCE) row_stats<T - 1>(r, nv, owned_row && owned_lane(), !edge);
             }
-            level<P, T + 1>(jj);
+            general_level<P, T + 1>(jj);
         }
     }
 
-    __device__ __forceinline__ void compute_row(const double* up, const double* ce,
-                                                const double* dn, int r,
-                                                const LaserSub& las, double* nv) {
+    __device__ __forceinline__ bool owned_lane() const {
+        return xl >= x0 && xl < x0 + ADV_WOUT && xl < p.c.nx;
+    }
+
+    __device__ __forceinline__ void compute_row_general(const double* up, const double* ce,
+                                                        const double* dn, int r,
+                                                        const LaserSub& las, double* nv) {
         const Coef& c = p.c;
         const int nx = c.nx, ny = c.ny;
         if (c.bc == 1 && (r == 0 || r == ny - 1)) {
@@ -250,104 +419,182 @@ struct WarpStrip {
             for (int v = 0; v < V; ++v) nv[v] = c.T_edge;
             return;
         }
-        // x neighbours across lanes: left of column 2l comes from lane l-1
-        // (or chunk q-1's lane 31), right of column 2l+1 from lane l+1.
-        double Lq[ADV_NCH], Rq[ADV_NCH];
-#pragma unroll
-        for (int q = 0; q < ADV_NCH; ++q) {
-            const double lc = (q > 0 && lane == 31) ? ce[2 * (q - 1) + 1] : ce[2 * q + 1];
-            const double rc = (q < ADV_NCH - 1 && lane == 0) ? ce[2 * (q + 1)] : ce[2 * q];
-            Lq[q] = __shfl_sync(0xffffffffu, lc, (lane + 31) & 31);
-            Rq[q] = __shfl_sync(0xffffffffu, rc, (lane + 1) & 31);
-        }
-        double L[V], R[V];
-#pragma unroll
-        for (int q = 0; q < ADV_NCH; ++q) {
-            L[2 * q] = Lq[q];          R[2 * q] = ce[2 * q + 1];
-            L[2 * q + 1] = ce[2 * q];  R[2 * q + 1] = Rq[q];
-        }
+        double Lo, Ro;
+        neighbours(ce, Lo, Ro);
+        double L[V] = {Lo, ce[0], ce[1], ce[2]};
+        double R[V] = {ce[1], ce[2], ce[3], Ro};
         if (edge) {
 #pragma unroll
             for (int v = 0; v < V; ++v) {
-                const int x = xs + 64 * (v >> 1) + 2 * lane + (v & 1);
-                if (x == 0) L[v] = ce[v];
-                if (x == nx - 1) R[v] = ce[v];
+                if (xl + v == 0) L[v] = ce[v];
+                if (xl + v == nx - 1) R[v] = ce[v];
             }
         }
         const double yd = __dsub_rn(__dmul_rn((double)r, c.dy), las.y_l);
         const double dy2 = __dmul_rn(yd, yd);
-        if (las.cs != 0.0 && dy2 < c.r2_cut) {
+        const bool src = las.cs != 0.0 && dy2 < c.r2_cut && src_strip;
+        double4 S4 = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (src) S4 = source4(xl, dy2, las.x_l, las.cs, c.dx, c.m2r, c.r2_cut);
+        const double S[V] = {S4.x, S4.y, S4.z, S4.w};
+        if (c.same_T) {
 #pragma unroll
-            for (int v = 0; v < V; ++v) {
-                const int x = xs + 64 * (v >> 1) + 2 * lane + (v & 1);
-                const double S = source_dt(x, dy2, las, c);
-                nv[v] = cell_update(ce[v], L[v], R[v], up[v], dn[v], S, c);
-            }
+            for (int v = 0; v < V; ++v)
+                nv[v] = src ? cell_core_src(ce[v], L[v], R[v], up[v], dn[v], S[v], h)
+                            : cell_core(ce[v], L[v], R[v], up[v], dn[v], h);
         } else {
 #pragma unroll
             for (int v = 0; v < V; ++v)
-                nv[v] = cell_update_nosrc(ce[v], L[v], R[v], up[v], dn[v], c);
+                nv[v] = cell_update(ce[v], L[v], R[v], up[v], dn[v], S[v], c);
         }
         if (edge && c.bc == 1) {
 #pragma unroll
-            for (int v = 0; v < V; ++v) {
-                const int x = xs + 64 * (v >> 1) + 2 * lane + (v & 1);
-                if (x == 0 || x == nx - 1) nv[v] = c.T_edge;
-            }
+            for (int v = 0; v < V; ++v)
+                if (xl + v == 0 || xl + v == nx - 1) nv[v] = c.T_edge;
         }
     }
 
     __device__ __forceinline__ void store_row(int r, const double* nv) {
-        double* dst = p.Tout + (size_t)r * p.c.nx;
+        double* dst = p.Tout + (size_t)r * p.c.nx + xl;
+        if constexpr (TMA) {
+            // even nx and a 4-aligned lane start: pairs share ownership
+            if (xl >= x0 && xl < x0 + ADV_WOUT) {
+                if (p.st256 && xl + 4 <= p.c.nx) {
+                    st_global_v4(dst, nv[0], nv[1], nv[2], nv[3]);
+                } else {
+                    if (xl < p.c.nx) *reinterpret_cast<double2*>(dst) = make_double2(nv[0], nv[1]);
+                    if (xl + 2 < p.c.nx)
+                        *reinterpret_cast<double2*>(dst + 2) = make_double2(nv[2], nv[3]);
+                }
+            }
+        } else {
 #pragma unroll
-        for (int q = 0; q < ADV_NCH; ++q) {
-            const int c0 = xs + 64 * q + 2 * lane;
-            if constexpr (TMA) {
-                // even nx and even c0: both cells of the pair share ownership
-                if (own[2 * q])
-                    *reinterpret_cast<double2*>(dst + c0) = make_double2(nv[2 * q], nv[2 * q + 1]);
-            } else {
-                if (own[2 * q]) dst[c0] = nv[2 * q];
-                if (own[2 * q + 1]) dst[c0 + 1] = nv[2 * q + 1];
+            for (int v = 0; v < V; ++v)
+                if (xl + v >= x0 && xl + v < x0 + ADV_WOUT && xl + v < p.c.nx) dst[v] = nv[v];
+        }
+    }
+
+    // Reduction, two tiers.  Every cell is tested against a per-box threshold
+    // thr = min(lane peak, Tm) (+inf for lanes owning no cell): one FP64
+    // compare folded into a predicate, no select.  Only a box in which some
+    // lane crossed its threshold -- the first box of a lane, or cells near
+    // the laser -- runs the exact pass: the crossed levels' rows are staged in
+    // shared memory and one compact routine updates the lane peak, its index
+    // and the molten rows.  NaN never crosses (strict '>'), as in the
+    // reference.
+    __device__ __forceinline__ void set_thresholds() {
+        const bool ol = owned_lane();
+#pragma unroll
+        for (int t = 0; t < K; ++t) {
+            const double tm = rs->tmx[t][lane];
+            const double a = (tm < p.c.Tm) ? tm : p.c.Tm;
+            thr[t] = ol ? a : INFINITY;
+        }
+    }
+
+    // full: the lane's four cells are all inside the grid.
+    template <int T>
+    __device__ __forceinline__ void row_stats(int r, const double* nv, bool own, bool full) {
+        bool hh = hit[T];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            if (full) hh = hh | (nv[v] > thr[T]);
+            else      hh = hh | (own && xl + v < p.c.nx && nv[v] > thr[T]);
+        }
+        hit[T] = hh;
+    }
+
+    // Copy level T's three box rows (slots of rows j-T .. j-T+2) to shared memory.
+    template <int T>
+    __device__ __forceinline__ void stage_level() {
+        if constexpr (T >= 1 && T < K) {
+            const double (&wn)[3][V] = win<T>();
+#pragma unroll
+            for (int P = 0; P < 3; ++P) {
+                double2* d = reinterpret_cast<double2*>(&rs->box[P][lane][0]);
+                d[0] = make_double2(wn[mod3(P - T)][0], wn[mod3(P - T)][1]);
+                d[1] = make_double2(wn[mod3(P - T)][2], wn[mod3(P - T)][3]);
             }
         }
     }
 
-    template <int T>
-    __device__ __forceinline__ void reduce_row(int r, const double* nv) {
-        // Row maximum over the lane's owned cells; fmax ignores NaN, as the
-        // reference's strict '>' does.  Ties resolve to the lowest column.
+    // Exact update of level t (1..K) from the box starting at row j; level-t
+    // rows come from the staging area (t < K) or from the stored field (t == K).
+    __device__ __forceinline__ void exact_level(int t, int j) {
+        const int nx = p.c.nx;
+        const bool ol = owned_lane();
         double m = -INFINITY;
+        for (int P = 0; P < 3; ++P) {
+            const int r = j + P - t;
+            const bool cand = r >= y0 && r < y1 && ol;
+            bool hot = false;
 #pragma unroll
-        for (int v = 0; v < V; ++v)
-            if (own[v]) m = fmax(m, nv[v]);
-        if (m > tmx[T]) {
-            int col = -1;
-#pragma unroll
-            for (int v = V - 1; v >= 0; --v)
-                if (own[v] && nv[v] == m) col = xs + 64 * (v >> 1) + 2 * lane + (v & 1);
-            tmx[T] = m;
-            targ[T] = (long long)r * p.c.nx + col;
+            for (int v = 0; v < V; ++v) {
+                const bool ok = cand && xl + v < nx;
+                double x = 0.0;
+                if (ok) x = (t < K) ? rs->box[P][lane][v] : p.Tout[(size_t)r * nx + xl + v];
+                m = (ok && x > m) ? x : m;
+                hot |= ok && x > p.c.Tm;
+            }
+            if (__any_sync(0xffffffffu, hot) && lane == 0) {
+                rs->ymn[t - 1] = min(rs->ymn[t - 1], r);
+                rs->ymx[t - 1] = max(rs->ymx[t - 1], r);
+            }
         }
-        if (m > p.c.Tm) {
-            ymn[T] = min(ymn[T], r);
-            ymx[T] = max(ymx[T], r);
+        if (m > rs->tmx[t - 1][lane]) {
+            long long arg = -1;
+            for (int P = 0; P < 3 && arg < 0; ++P) {
+                const int r = j + P - t;
+                if (!(r >= y0 && r < y1 && ol)) continue;
+                for (int v = 0; v < V; ++v) {
+                    if (xl + v >= nx) break;
+                    const double x = (t < K) ? rs->box[P][lane][v] : p.Tout[(size_t)r * nx + xl + v];
+                    if (x == m) { arg = (long long)r * nx + xl + v; break; }
+                }
+            }
+            rs->tmx[t - 1][lane] = m;
+            rs->arg[t - 1][lane] = arg;
+        }
+    }
+
+    __device__ __forceinline__ void resolve_box(int j) {
+        unsigned bits = 0;
+#pragma unroll
+        for (int t = 0; t < K; ++t) {
+            bits |= hit[t] ? (1u << t) : 0u;
+            hit[t] = false;
+        }
+        bits = __reduce_or_sync(0xffffffffu, bits);
+        if (bits == 0u) return;
+        for (int t = 1; t <= K; ++t) {
+            if (!((bits >> (t - 1)) & 1u)) continue;
+            switch (t) {               // stage level t's rows from its registers
+                case 1: stage_level<1>(); break;
+                case 2: stage_level<2>(); break;
+                case 3: stage_level<3>(); break;
+                default: break;
+            }
+            __syncwarp();
+            exact_level(t, j);
+            __syncwarp();
         }
     }
 };
 
+template <int K>
+struct AdvOcc { static constexpr int min_ctas = (K <= 2) ? 4 : 3; };
+
 template <int K, bool TMA, bool REDUCE>
-__global__ void __launch_bounds__(ADV_WARPS * 32, 3)
+__global__ void __launch_bounds__(ADV_WARPS * 32, AdvOcc<K>::min_ctas)
 advance_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ AdvParams p) {
-    using G = AdvGeo<K>;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ Partial red[ADV_WARPS][K];
     __shared__ unsigned int s_last;
+    __shared__ __align__(16) RedSmem<K> s_red[REDUCE ? ADV_WARPS : 1];
 
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double* stages = reinterpret_cast<double*>(smem) + wid * (ADV_S * G::STAGE_DOUBLES);
+    double* stages = reinterpret_cast<double*>(smem) + wid * (ADV_S * ADV_STAGE_DOUBLES);
     uint64_t* bars = reinterpret_cast<uint64_t*>(
-        smem + size_t(ADV_WARPS) * ADV_S * G::STAGE_DOUBLES * sizeof(double)) + wid * ADV_S;
+        smem + size_t(ADV_WARPS) * ADV_S * ADV_STAGE_DOUBLES * sizeof(double)) + wid * ADV_S;
 
     if constexpr (TMA) {
         if (lane == 0) {
@@ -358,22 +605,37 @@ advance_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
         __syncwarp();
     }
 
-    uint32_t gbox = 0;
-    WarpStrip<K, TMA, REDUCE> ws(p, &map, stages, bars, gbox, lane);
-    for (int task = blockIdx.x * ADV_WARPS + wid; task < p.ntasks;
-         task += gridDim.x * ADV_WARPS) {
-        ws.run_task(task);
-        if (ws.failed) break;
+    WarpStrip<K, TMA, REDUCE> ws(p, &map, stages, bars, lane, &s_red[REDUCE ? wid : 0]);
+    if (p.tasks) {
+        // dynamic: lane 0 draws the next task for the warp
+        for (;;) {
+            unsigned int t = 0;
+            if (lane == 0) t = atomicAdd(p.tasks, 1u);
+            t = __shfl_sync(0xffffffffu, t, 0);
+            if (t >= (unsigned int)p.ntasks) break;
+            ws.run_task((int)t);
+            if (ws.failed) break;
+        }
+    } else {
+        for (int task = blockIdx.x * ADV_WARPS + wid; task < p.ntasks;
+             task += gridDim.x * ADV_WARPS) {
+            ws.run_task(task);
+            if (ws.failed) break;
+        }
     }
 
+    const long long N = (long long)p.c.nx * p.c.ny;
     if constexpr (REDUCE) {
 #pragma unroll
+        __syncwarp();
         for (int t = 0; t < K; ++t) {
-            partial_warp_reduce(ws.tmx[t], ws.targ[t], ws.ymn[t], ws.ymx[t]);
-            if (lane == 0) red[wid][t] = Partial{ws.tmx[t], ws.targ[t], ws.ymn[t], ws.ymx[t]};
+            double tm = s_red[wid].tmx[t][lane];
+            long long ag = s_red[wid].arg[t][lane];
+            int mn = s_red[wid].ymn[t], mx = s_red[wid].ymx[t];
+            partial_warp_reduce(tm, ag, mn, mx);
+            if (lane == 0) red[wid][t] = Partial{tm, ag, mn, mx};
         }
         __syncthreads();
-        const long long N = (long long)p.c.nx * p.c.ny;
         if (threadIdx.x < K) {
             const int t = threadIdx.x;
             double tm = -1.0; long long ag = N; int mn = p.c.ny, mx = -1;
@@ -381,7 +643,7 @@ advance_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
                 partial_take(tm, ag, mn, mx, red[w][t].tmax, red[w][t].arg,
                              red[w][t].ymin, red[w][t].ymax);
             if (p.ref_out) p.ref_out[blockIdx.x] = Partial{tm, ag, mn, mx};
-            else p.scratch[(size_t)blockIdx.x * K + t] = Partial{tm, ag, mn, mx};
+            else if (p.ring) p.scratch[(size_t)blockIdx.x * K + t] = Partial{tm, ag, mn, mx};
         }
         if (p.ref_out) {
             // Reference layout: the caller finalizes ref_nparts entries, so
@@ -390,35 +652,43 @@ advance_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
             for (long long i = gridDim.x + (long long)blockIdx.x * blockDim.x + threadIdx.x;
                  i < p.ref_nparts; i += (long long)gridDim.x * blockDim.x)
                 p.ref_out[i] = neutral;
-            return;
         }
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0)
-            s_last = (atomicAdd(p.counter, 1u) == gridDim.x - 1) ? 1u : 0u;
-        __syncthreads();
-        if (!s_last) return;
-        __threadfence();
-        for (int t = 0; t < K; ++t) {
-            double tm = -1.0; long long ag = N; int mn = p.c.ny, mx = -1;
-            for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
-                const Partial* q = &p.scratch[(size_t)i * K + t];
-                partial_take(tm, ag, mn, mx, __ldcg(&q->tmax), __ldcg(&q->arg),
-                             __ldcg(&q->ymin), __ldcg(&q->ymax));
-            }
-            partial_warp_reduce(tm, ag, mn, mx);
-            __syncthreads();
-            if (lane == 0) red[wid][0] = Partial{tm, ag, mn, mx};
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                double a = -1.0; long long b = N; int c1 = p.c.ny, d1 = -1;
-                for (int w = 0; w < ADV_WARPS; ++w)
-                    partial_take(a, b, c1, d1, red[w][0].tmax, red[w][0].arg,
-                                 red[w][0].ymin, red[w][0].ymax);
-                p.ring[t] = Partial{a, b, c1, d1};
+    }
+    if (!p.counter) return;
+    // Last CTA: finalize the per-step Partials and re-arm the counters.
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+        s_last = (atomicAdd(p.counter, 1u) == gridDim.x - 1) ? 1u : 0u;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if constexpr (REDUCE) {
+        if (p.ring) {
+            for (int t = 0; t < K; ++t) {
+                double tm = -1.0; long long ag = N; int mn = p.c.ny, mx = -1;
+                for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+                    const Partial* q = &p.scratch[(size_t)i * K + t];
+                    partial_take(tm, ag, mn, mx, __ldcg(&q->tmax), __ldcg(&q->arg),
+                                 __ldcg(&q->ymin), __ldcg(&q->ymax));
+                }
+                partial_warp_reduce(tm, ag, mn, mx);
+                __syncthreads();
+                if (lane == 0) red[wid][0] = Partial{tm, ag, mn, mx};
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    double a = -1.0; long long b = N; int c1 = p.c.ny, d1 = -1;
+                    for (int w = 0; w < ADV_WARPS; ++w)
+                        partial_take(a, b, c1, d1, red[w][0].tmax, red[w][0].arg,
+                                     red[w][0].ymin, red[w][0].ymax);
+                    p.ring[t] = Partial{a, b, c1, d1};
+                }
             }
         }
-        if (threadIdx.x == 0) *p.counter = 0u;
+    }
+    if (threadIdx.x == 0) {
+        *p.counter = 0u;
+        if (p.tasks) *p.tasks = 0u;
     }
 }
 

@@ -81,32 +81,27 @@ inline LaserSub make_laser(const StepConst& k, double x_l, double y_l, double q_
     return l;
 }
 
-// Loss increment dt*loss(T)/... for one cell.
+// dt-scaled loss of one cell.  The multiplies are spelled out so that the
+// radiation difference is exactly zero at T = Tamb (Tamb4 is formed the same
+// way on the host).
 __device__ __forceinline__ double loss_dt(double T, const Coef& c) {
-    const double da = T - c.Tamb;
-    const double t2 = T * T;
-    const double e4 = t2 * t2 - c.Tamb4;
+    const double da = __dsub_rn(T, c.Tamb);
+    const double t2 = __dmul_rn(T, T);
+    const double e4 = __dsub_rn(__dmul_rn(t2, t2), c.Tamb4);
     double lin;
-    if (c.same_T) lin = c.c_ls * da;
-    else          lin = fma(c.c_sub, T - c.Tsub, c.c_conv * da);
+    if (c.same_T) lin = __dmul_rn(c.c_ls, da);
+    else          lin = fma(c.c_sub, __dsub_rn(T, c.Tsub), __dmul_rn(c.c_conv, da));
     return fma(c.c_rad, e4, lin);
 }
 
-// Baseline update of one interior-formula cell; S_dt already dt-scaled.
+// Baseline update of one cell (general Tamb != Tsub form); S_dt dt-scaled.
 __device__ __forceinline__ double cell_update(double T, double L, double R,
                                               double U, double D, double S_dt,
                                               const Coef& c) {
     const double lx = fma(-2.0, T, R + L);
     const double ly = fma(-2.0, T, U + D);
-    const double inc = fma(c.ax, lx, c.ay * ly);
-    return T + ((inc + S_dt) - loss_dt(T, c));
-}
-__device__ __forceinline__ double cell_update_nosrc(double T, double L, double R,
-                                                    double U, double D, const Coef& c) {
-    const double lx = fma(-2.0, T, R + L);
-    const double ly = fma(-2.0, T, U + D);
-    const double inc = fma(c.ax, lx, c.ay * ly);
-    return T + (inc - loss_dt(T, c));
+    const double inc = fma(c.ax, lx, __dmul_rn(c.ay, ly));
+    return __dadd_rn(T, __dsub_rn(__dadd_rn(inc, S_dt), loss_dt(T, c)));
 }
 
 // Gaussian source increment at column x of a row whose (y - y_l)^2 is dy2.

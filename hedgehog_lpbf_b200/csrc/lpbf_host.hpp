@@ -20,9 +20,10 @@ constexpr int MAX_CTAS = 2048;     // most CTAs a reducing launch may use
 // Device workspace.  The counter and error word sit in the first 256 bytes;
 // per-CTA partials follow.
 struct Workspace {
-    unsigned int counter;
-    unsigned int err;
-    unsigned int pad[62];
+    unsigned int counter;          // last-CTA ticket
+    unsigned int err;              // error word
+    unsigned int tasks;            // dynamic task counter
+    unsigned int pad[61];
     Partial parts[MAX_CTAS * KMAX];
 };
 static_assert(offsetof(Workspace, parts) == 256, "workspace header");
