@@ -94,6 +94,28 @@ int lpbf_b200_advance_launches(int nx, int ny, int n_steps, const lpbf_b200_opts
  * a TMA wait exceeded its time limit and the launch stopped early. */
 int lpbf_b200_read_error(const void* work, cudaStream_t stream, unsigned int* err);
 
+/* No counterpart in the reference.  lpbf_b200_advance without a workspace,
+ * for callers that cannot allocate device memory: code running inside a
+ * device-memory budget fixed at start-up, bindings that only pass raw device
+ * pointers (cgo, JNI) and own no allocator, hosts where a cudaMalloc would
+ * synchronize the device at a forbidden point.  Its scratch is a fixed
+ * LPBF_B200_NOALLOC_SCRATCH_BYTES array in the library's device memory, held
+ * by every GPU that loads the library until the process exits.
+ *  - The first call on a device looks up that array's device address
+ *    (cudaGetSymbolAddress) and caches it; make that first call before any
+ *    stream capture.
+ *  - Every call clears and reuses the same array: calls that overlap on the
+ *    GPU (other streams, other threads) race and must not be issued.
+ *  - Baseline physics only (phys == 1 returns LPBF_ERR_UNSUPPORTED); a GPU
+ *    needing more than 4096 per-CTA partial records for the requested depth
+ *    is rejected with LPBF_ERR_WORKSPACE.
+ * Inputs, outputs and results are as for lpbf_b200_advance. */
+#define LPBF_B200_NOALLOC_SCRATCH_BYTES 98560
+int lpbf_b200_advance_noalloc(double* T_a, double* T_b, const StepConst* k,
+                              const lpbf_tick* plan, int n_steps,
+                              const lpbf_b200_opts* opts, Partial* ring,
+                              cudaStream_t stream, int* result_in_b);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
