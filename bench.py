@@ -206,7 +206,7 @@ def run_b200_arm(args, rank, world, local_rank):
     torch.cuda.set_device(dev)
     mat, pr, dom, k, plan = workload(rank)
     s = Solver(k, device=dev, Tm=mat.Tm, depth=args.depth)
-    depth = min(4, args.depth) if args.depth > 0 else (4 if N_SIDE * N_SIDE >= (1 << 22) else 2)
+    depth = min(4, args.depth) if args.depth > 0 else (3 if N_SIDE * N_SIDE >= (1 << 22) else 2)
     launches = s.launches(STEPS_PER_ITER)
     ring = s.new_ring(STEPS_PER_ITER)
     stream = torch.cuda.current_stream()

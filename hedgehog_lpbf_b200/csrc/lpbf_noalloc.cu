@@ -78,7 +78,7 @@ extern "C" int lpbf_b200_advance_noalloc(double* T_a, double* T_b, const StepCon
     int depth = opts->depth;
     if (depth <= 0) {
         const long long n = (long long)k->nx * k->ny;
-        depth = (n >= (1ll << 22)) ? 4 : (n >= (1ll << 18)) ? 2 : 1;
+        depth = (n >= (1ll << 22)) ? 3 : (n >= (1ll << 18)) ? 2 : 1;
     }
     depth = std::min(std::max(depth, 1), 4);
     // Reject configurations whose per-CTA partials would not fit the scratch.
