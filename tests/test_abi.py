@@ -66,3 +66,16 @@ def test_headers_compile_and_link(tmp_path, lang):
                    check=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
     assert out.split()[0] == "1"
+
+
+def test_gpu_step_task_header_builds_against_library():
+    """include/gpu_step_task.hpp compiles (hh-compat) and links to the library;
+    with the reference tree present, so does the reference's own
+    hh_gpu_main.cpp against these headers."""
+    d = os.path.join(ROOT, "tests", "dropin")
+    subprocess.run(["make", "-s", "-C", d, "demo"], check=True)
+    assert os.path.exists(os.path.join(ROOT, "tests", "_build", "gpu_task_demo"))
+    ref = os.environ.get("LPBF_REFERENCE", "/root/reference")
+    if os.path.isdir(os.path.join(ref, "src", "gpu")):
+        subprocess.run(["make", "-s", "-C", d, "ref", f"REF={ref}"], check=True)
+        assert os.path.exists(os.path.join(ROOT, "tests", "_build", "ref_hhcuda_on_b200"))

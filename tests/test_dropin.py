@@ -1,0 +1,120 @@
+# SPDX-License-Identifier: 0BSD
+"""Drop-in: the Hedgehog GPU step graph (include/gpu_step_task.hpp) on
+liblpbf_b200 reproduces the reference's case-0 outputs.
+
+* tests/dropin/gpu_task_demo.cpp drives the graph in every mode of the
+  reference task (0, 1, 2 unfused, 2 fused with several depths, pinned,
+  odd batch sizes); all must write the same metrics.csv, equal to the
+  reference's committed reference/case0/metrics.csv at its precision, and
+  fields and running maxima that match the oracle.
+* When built (needs the reference tree at build time), the reference's own
+  src/gpu/hh_gpu_main.cpp compiled against these headers and this library
+  must write the same metrics.csv.
+"""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from hedgehog_lpbf_b200 import params as P
+from hedgehog_lpbf_b200 import plan as PL
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BUILD = os.path.join(ROOT, "tests", "_build")
+GOLD = os.path.join(ROOT, "tests", "golden", "case0.json")
+
+
+def _demo():
+    exe = os.path.join(BUILD, "gpu_task_demo")
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "tests", "dropin"), "demo"], check=True)
+    return exe
+
+
+def _golden_rows():
+    g = json.load(open(GOLD))
+    return [[r["step"], r["t_us"], r["x_laser_um"], r["peakT_K"], r["W_um"]] for r in g["metrics"]], g
+
+
+def _csv_rows(path):
+    lines = open(path).read().strip().splitlines()
+    assert lines[0] == "step,t_us,x_laser_um,peakT_K,W_um"
+    return [[float(v) for v in ln.split(",")] for ln in lines[1:]]
+
+
+def _fmt(v):
+    return "%.6g" % v
+
+
+@pytest.fixture(scope="module")
+def oracle_case0():
+    """Oracle run of case 0 with the reference metrics (GPU-reduce semantics)."""
+    mat, dom = P.Material(), P.Domain()
+    pr = P.apply_case("0", P.Process())
+    dt = P.dt_cfl(mat, dom)
+    n = int(1.5e-3 / dt)
+    k = P.make_const(mat, pr, dom, dt)
+    plan = PL.single_track(pr, dom, dt, n, snap_every=200)
+    las = PL.laser_array(plan)
+    T = np.full(dom.nx * dom.ny, pr.Tamb)
+    peak_T, peak_W, steady = 0.0, 0.0, 0.0
+    for s in range(n):
+        k.x_l, k.y_l, k.q_scale = las[s]
+        T = O.step(T, k)
+        tmax, arg, ymin, ymax = O.reduce(T, dom.nx, dom.ny, mat.Tm)
+        W = 0.0 if ymax < 0 else (ymax - ymin + 1) * dom.dy() * 1e6
+        peak_T, peak_W = max(peak_T, tmax), max(peak_W, W)
+        cruise = (not plan["wrapped"][s]) and 0.45 * dom.Lx <= plan["x_laser_csv"][s] <= 0.85 * dom.Lx
+        if cruise and tmax > mat.Tm:
+            col = T.reshape(dom.ny, dom.nx)[:, arg % dom.nx]
+            steady = max(steady, O.w_sub(col, dom.dy(), mat.Tm))
+    return dict(T=T, peak_T=peak_T, peak_W=peak_W, steady=steady, n=n)
+
+
+RUNS = [  # mode, fused, pinned, batch, depth
+    (0, 0, 0, 64, 0), (1, 0, 0, 64, 0), (2, 0, 0, 64, 0), (2, 1, 0, 64, 0),
+    (2, 1, 1, 7, 3), (2, 1, 0, 100, 4), (2, 1, 0, 1, 2),
+]
+
+
+def test_gpu_step_task_all_modes_match_reference_case0(gpu, tmp_path, oracle_case0):
+    exe = _demo()
+    want, g = _golden_rows()
+    csvs = []
+    for mode, fused, pinned, batch, depth in RUNS:
+        out = tmp_path / f"m{mode}f{fused}p{pinned}b{batch}d{depth}"
+        subprocess.run([exe, str(out), str(mode), str(fused), str(pinned), str(batch), str(depth)],
+                       check=True, timeout=300)
+        text = open(out / "metrics.csv").read()
+        csvs.append(text)
+        rows = _csv_rows(out / "metrics.csv")
+        assert [[_fmt(v) for v in r] for r in rows] == [[_fmt(v) for v in r] for r in want]
+        pk_T, pk_W, steady, n = open(out / "summary.txt").read().split()
+        o = oracle_case0
+        assert int(n) == o["n"] == g["meta"]["n_steps"]
+        assert abs(float(pk_T) - o["peak_T"]) <= 1e-12 * o["peak_T"]
+        assert float(pk_W) == o["peak_W"]
+        assert abs(float(steady) - o["steady"]) <= 1e-9 * o["steady"]
+        T = np.fromfile(out / f"T_step_{o['n'] - 1:06d}.bin", dtype=np.float64)
+        assert np.max(np.abs(T - o["T"]) / np.maximum(np.abs(o["T"]), 1.0)) <= 1e-12
+    assert all(c == csvs[0] for c in csvs), "metrics.csv differs between modes"
+    assert _fmt(float(oracle_case0["peak_T"])) == _fmt(g["meta"]["peak_T_K"])
+
+
+def test_reference_driver_on_this_library(gpu, tmp_path):
+    exe = os.path.join(BUILD, "ref_hhcuda_on_b200")
+    if not os.path.exists(exe):
+        pytest.skip("reference driver not built (needs the reference tree at build time)")
+    want, g = _golden_rows()
+    for extra in ([], ["--fused"], ["--mode=0"], ["--batch=5", "--pinned", "--fused"]):
+        out = tmp_path / ("run" + "".join(e.strip("-=") for e in extra))
+        subprocess.run([exe, "--case=0", f"--out={out}", "--snap-every=200", *extra],
+                       check=True, timeout=300, capture_output=True)
+        rows = _csv_rows(out / "metrics.csv")
+        assert [[_fmt(v) for v in r] for r in rows] == [[_fmt(v) for v in r] for r in want]
+        meta = json.load(open(out / "meta.json"))
+        assert _fmt(meta["peak_T_K"]) == _fmt(g["meta"]["peak_T_K"])
+        assert _fmt(meta["peak_W_um"]) == _fmt(g["meta"]["peak_W_um"])
