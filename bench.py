@@ -235,6 +235,7 @@ def run_b200_arm(args, rank, world, local_rank):
     barrier()
     ms = ev0.elapsed_time(ev1)
     step_ms = [step_ev[i].elapsed_time(step_ev[i + 1]) for i in range(args.steps)]
+    T64 = s.field.clone() if args.f32k else None
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -268,6 +269,31 @@ def run_b200_arm(args, rank, world, local_rank):
         dist.all_reduce(t2, op=dist.ReduceOp.MAX)
     e2e_value = cells * STEPS_PER_ITER * e2e_steps * world / (float(t2.item()) * 1e-3) / 1e9
 
+    # ---- FP32 compensated variant on the same plan, against the FP64 field --
+    f32k = None
+    if args.f32k:
+        from hedgehog_lpbf_b200.solver import SolverF32K
+        del host_in, host_out
+        sk = SolverF32K(k, device=dev, Tm=mat.Tm, depth=args.depth)
+        for i in range(args.warmup):
+            sk.advance(plan_slice(plan, i), ring)
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for i in range(args.steps):
+            sk.advance(plan_slice(plan, args.warmup + i), ring)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        fms = f0.elapsed_time(f1)
+        err = float((sk.field64() - T64).abs().max().item())
+        f32k = {"value": cells * STEPS_PER_ITER * args.steps / (fms * 1e-3) / 1e9,
+                "unit": "GCell-updates/s", "ms_per_step": fms / args.steps,
+                "time_steps": STEPS_PER_ITER * (args.warmup + args.steps),
+                "max_abs_err_vs_fp64_K": err, "target_K": 0.05,
+                "bytes_per_update": 16}
+        del sk, T64
+
     if rank != 0:
         return
     peak, peak_src = measured_peaks()
@@ -294,6 +320,7 @@ def run_b200_arm(args, rank, world, local_rank):
                 "d2h_bytes_per_step": cells * 8 + STEPS_PER_ITER * 24,
                 "steps": e2e_steps},
         "gpu_launches": launches * args.steps,
+        "f32k": f32k,
         "clocks": clk.summary(),
         "error_word": err,
     }
@@ -313,6 +340,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=15.0,
                     help="seconds of CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-f32k", dest="f32k", action="store_false",
+                    help="skip the FP32 compensated leg")
     ap.add_argument("--side", type=int, default=N_SIDE,
                     help="grid side (smaller sides are for profiling only)")
     ap.add_argument("--iter-steps", type=int, default=STEPS_PER_ITER,

@@ -103,30 +103,6 @@ bool tensor_map_f32(const void* base, int nx, int ny, int box_cols, int box_rows
 // ---- launch of one temporally blocked step ---------------------------------
 namespace {
 
-// Rows whose source term can be non-zero in any of the K substeps (a
-// superset: the kernel decides exactly, this only routes rows to the general
-// body).  Empty when every substep has the beam off.
-void laser_band(const Coef& c, const LaserSub* las, int K, int* lo, int* hi, int* xlo,
-                int* xhi) {
-    int blo = 1 << 30, bhi = -(1 << 30), cxlo = 1 << 30, cxhi = -(1 << 30);
-    const double R = std::sqrt(c.r2_cut);
-    for (int t = 0; t < K; ++t) {
-        if (las[t].cs == 0.0) continue;
-        const double y = las[t].y_l, x = las[t].x_l;
-        if (!std::isfinite(y) || !std::isfinite(x) || !std::isfinite(R) || c.dy <= 0.0 ||
-            c.dx <= 0.0) {
-            blo = -2; bhi = c.ny + 2; cxlo = -2; cxhi = c.nx + 2;
-            break;
-        }
-        auto clampi = [](double v, double a, double b) { return (int)std::max(a, std::min(v, b)); };
-        blo = std::min(blo, clampi(std::floor((y - R) / c.dy) - 2.0, -2.0, c.ny + 2.0));
-        bhi = std::max(bhi, clampi(std::ceil((y + R) / c.dy) + 2.0, -2.0, c.ny + 2.0));
-        cxlo = std::min(cxlo, clampi(std::floor((x - R) / c.dx) - 2.0, -2.0, c.nx + 2.0));
-        cxhi = std::max(cxhi, clampi(std::ceil((x + R) / c.dx) + 2.0, -2.0, c.nx + 2.0));
-    }
-    *lo = blo; *hi = bhi; *xlo = cxlo; *xhi = cxhi;
-}
-
 template <int K, bool TMA, bool REDUCE>
 cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const LaserSub* las,
                      Partial* ring, Workspace* ws, Partial* ref_out, long long ref_nparts,

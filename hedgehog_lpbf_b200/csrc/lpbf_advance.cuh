@@ -115,7 +115,7 @@ __device__ __forceinline__ double cell_core_src(double T, double L, double R, do
 
 // Gaussian source increment of a lane's four cells starting at column x0
 // (out of line: the exp code exists once in the binary).
-__device__ __noinline__ double4 source4(int x0, double dy2, double x_l, double cs, double dx,
+static __device__ __noinline__ double4 source4(int x0, double dy2, double x_l, double cs, double dx,
                                         double m2r, double r2_cut) {
     double S[4];
 #pragma unroll

@@ -94,6 +94,23 @@ int lpbf_b200_advance_launches(int nx, int ny, int n_steps, const lpbf_b200_opts
  * a TMA wait exceeded its time limit and the launch stopped early. */
 int lpbf_b200_read_error(const void* work, cudaStream_t stream, unsigned int* err);
 
+/* FP32 compensated variant (no reference counterpart; the reference path is
+ * FP64 only).  The field is two f32 arrays, hi and lo, with T = hi + lo; each
+ * step adds its increment with an error-free two-sum and keeps the rounding
+ * error in lo, the Gaussian source is evaluated in FP64, and per-step Partials
+ * are reduced on hi + lo in FP64.  (hi_a, lo_a) holds the start field,
+ * (hi_b, lo_b) the other half of the ping-pong pair; *result_in_b as for
+ * lpbf_b200_advance.  Requires nx % 4 == 0 and 16-byte aligned arrays
+ * (LPBF_ERR_UNSUPPORTED otherwise) and baseline physics.  Needs a workspace. */
+int lpbf_b200_advance_f32k(float* hi_a, float* lo_a, float* hi_b, float* lo_b,
+                           const StepConst* k, const lpbf_tick* plan, int n_steps,
+                           const lpbf_b200_opts* opts, Partial* ring, void* work,
+                           size_t work_bytes, cudaStream_t stream, int* result_in_b);
+/* hi = (float)T, lo = (float)(T - hi), and back: T = (double)hi + (double)lo. */
+int lpbf_b200_f32k_split(const double* T, float* hi, float* lo, size_t n, cudaStream_t stream);
+int lpbf_b200_f32k_join(const float* hi, const float* lo, double* T, size_t n,
+                        cudaStream_t stream);
+
 /* No counterpart in the reference.  lpbf_b200_advance without a workspace,
  * for callers that cannot allocate device memory: code running inside a
  * device-memory budget fixed at start-up, bindings that only pass raw device
