@@ -28,6 +28,22 @@ class Opts(ctypes.Structure):
                 ("Tm", ctypes.c_double), ("depth", ctypes.c_int), ("rows", ctypes.c_int)]
 
 
+class Scenario(ctypes.Structure):
+    """lpbf_b200_scenario (include/lpbf_b200.h)."""
+    _fields_ = [("k", ctypes.POINTER(StepConst)), ("plan", _vp), ("T_a", _vp), ("T_b", _vp),
+                ("ring", _vp), ("bc", ctypes.c_int), ("T_edge", ctypes.c_double),
+                ("Tm", ctypes.c_double)]
+
+
+class BatchOpts(ctypes.Structure):
+    """lpbf_b200_batch_opts (include/lpbf_b200.h)."""
+    _fields_ = [("depth", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
+                ("rows", ctypes.c_int * 4), ("staging", ctypes.c_int)]
+
+
+_sp = ctypes.POINTER(Scenario)
+_bop = ctypes.POINTER(BatchOpts)
+
 # name -> (restype, argtypes); every symbol the headers in include/ declare.
 SIGNATURES = {
     # include/lpbf_kernels.hpp (reference drop-in)
@@ -58,6 +74,17 @@ SIGNATURES = {
     "lpbf_b200_advance_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(StepConst), _vp,
                                                  ctypes.c_int, ctypes.POINTER(Opts), _vp, _vp,
                                                  ctypes.POINTER(ctypes.c_int)]),
+    "lpbf_b200_batch_size_class": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "lpbf_b200_batch_workspace_bytes": (ctypes.c_size_t, [_sp, ctypes.c_int, ctypes.c_int, _bop]),
+    "lpbf_b200_batch_create": (ctypes.c_int, [_sp, ctypes.c_int, ctypes.c_int, _bop, _vp,
+                                              ctypes.c_size_t, _vp, ctypes.POINTER(_vp)]),
+    "lpbf_b200_batch_run": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    "lpbf_b200_batch_result_in_b": (ctypes.c_int, [_vp]),
+    "lpbf_b200_batch_launches": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "lpbf_b200_batch_tasks": (ctypes.c_int, [_vp]),
+    "lpbf_b200_batch_scenario_rows": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "lpbf_b200_batch_read_error": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_uint)]),
+    "lpbf_b200_batch_destroy": (None, [_vp]),
 }
 
 
@@ -97,4 +124,5 @@ def check(status: int, what: str = "liblpbf_b200") -> None:
         raise RuntimeError(f"{what}: status {status} ({msg})")
 
 
-__all__ = ["lib", "lib_path", "check", "Opts", "SIGNATURES", "StepConst", "Partial", "Tick"]
+__all__ = ["lib", "lib_path", "check", "Opts", "Scenario", "BatchOpts", "SIGNATURES", "StepConst",
+           "Partial", "Tick"]

@@ -127,16 +127,19 @@ static __device__ __noinline__ double4 source4(int x0, double dy2, double x_l, d
     return make_double4(S[0], S[1], S[2], S[3]);
 }
 
+// 32-byte stores of level-K values.  They carry no "memory" clobber: the
+// kernel never reads the destination field back (the exact reduction reads
+// staged copies), and a clobber would make the compiler reload every
+// parameter it keeps in memory after each store.
 __device__ __forceinline__ void st_global_v4(double* p, double a, double b, double c, double d) {
     asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};"
-                 :: "l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+                 :: "l"(p), "d"(a), "d"(b), "d"(c), "d"(d));
 }
 // 32-byte store issued under a predicate (no branch).
 __device__ __forceinline__ void st_global_v4_pred(double* p, const double* v, bool pred) {
     asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %5, 0;\n\t"
                  "@q st.global.v4.f64 [%0], {%1, %2, %3, %4};\n\t}"
-                 :: "l"(p), "d"(v[0]), "d"(v[1]), "d"(v[2]), "d"(v[3]), "r"((int)pred)
-                 : "memory");
+                 :: "l"(p), "d"(v[0]), "d"(v[1]), "d"(v[2]), "d"(v[3]), "r"((int)pred));
 }
 
 // Per-warp reduction state in shared memory: lane peaks and their flat
@@ -152,7 +155,13 @@ struct alignas(16) RedSmem {
 static_assert(offsetof(RedSmem<1>, box) % 16 == 0 && sizeof(RedSmem<1>) % 16 == 0, "align");
 static_assert(offsetof(RedSmem<3>, box) % 16 == 0 && sizeof(RedSmem<3>) % 16 == 0, "align");
 
-template <int K, bool TMA, bool REDUCE>
+// TMA: rows are staged in shared memory by the copy engine (otherwise each
+// lane loads its cells directly).  BULK: the staging copies are plain bulk
+// copies, one per row, instead of tensor-map loads: no descriptor is read per
+// copy, which matters when warps work on many different fields at once (a
+// tensor map in global memory is fetched by the copy engine); requires an
+// even row length and a 16-byte aligned field.
+template <int K, bool TMA, bool REDUCE, bool BULK = false>
 struct WarpStrip {
     static constexpr int V = ADV_V;
 
@@ -162,10 +171,12 @@ struct WarpStrip {
     uint64_t* bars;                // this warp's S mbarriers
     uint32_t gbox;                 // running box counter (mbarrier phase tracking)
     const int lane;
-    const HotCoef h;
+    HotCoef h;
 
     int x0, xs, xl, y0, y1, jy0, jend, nbox, issued;
+    int last_chunk;                      // row chunk of this warp's previous task (-1: none)
     bool edge, failed, own_all, src_strip;
+    bool incl;                           // this task also examines values equal to the lane peak
 
     double w0[3][V];                     // level-0 window (slot = row % 3)
     double w[K > 1 ? K - 1 : 1][3][V];   // windows of levels 1..K-1
@@ -174,14 +185,30 @@ struct WarpStrip {
     // row extent, and in shared memory the flat index of the lane's peak.
     double thr[K];                       // per-box trigger: min(peak, Tm), +inf off-strip
     bool hit[K];                         // a cell of this box crossed thr
+    unsigned kmask;                      // level-K rows of this box staged in rs->box
     RedSmem<K>* rs;                      // this warp's reduction state (shared memory)
 
+    // gbox0: boxes this warp has already consumed through its stage ring
+    // (mbarrier phases continue across WarpStrip instances of one warp).
     __device__ __forceinline__ WarpStrip(const AdvParams& p_, const CUtensorMap* m,
-                                         double* st, uint64_t* b, int ln, RedSmem<K>* rs_)
-        : p(p_), map(m), stages(st), bars(b), gbox(0), lane(ln),
+                                         double* st, uint64_t* b, int ln, RedSmem<K>* rs_,
+                                         uint32_t gbox0 = 0)
+        : p(p_), map(m), stages(st), bars(b), gbox(gbox0), lane(ln),
           h{p_.c.ax, p_.c.ay, p_.c.c_ls, p_.c.c_rad, p_.c.Tamb, p_.c.Tamb4},
-          failed(false), rs(rs_) {
+          last_chunk(-1), failed(false), incl(false), kmask(0u), rs(rs_) {
+        reset_red();
+    }
+
+    // Re-read the hot coefficients after the parameters behind `p` changed
+    // (the batched kernel rebinds one WarpStrip to another field per task).
+    __device__ __forceinline__ void reload_coef() {
+        h = HotCoef{p.c.ax, p.c.ay, p.c.c_ls, p.c.c_rad, p.c.Tamb, p.c.Tamb4};
+    }
+
+    // Neutral reduction state for every level (a new field for this warp).
+    __device__ __forceinline__ void reset_red() {
         const long long N = (long long)p.c.nx * p.c.ny;
+        last_chunk = -1;
         if constexpr (REDUCE) {
 #pragma unroll
             for (int t = 0; t < K; ++t) {
@@ -198,14 +225,37 @@ struct WarpStrip {
         const uint32_t g = gbox + b;
         const int st = g % ADV_S;
         double* dst = stages + st * ADV_STAGE_DOUBLES;
-        mbar_expect_tx(&bars[st], ADV_STAGE_DOUBLES * sizeof(double));
-        tma_load_2d(dst, map, xs, jy0 + b * ADV_R, &bars[st]);
+        if constexpr (BULK) {
+            // The rows of the box that exist, columns clipped to the field;
+            // stage words outside stay stale and are never used (rows past
+            // the end are not read, columns off the field are mirror-edge
+            // halo whose values reach no owned cell).
+            const int nx = p.c.nx;
+            const int r0 = jy0 + b * ADV_R;
+            const int nr = min(ADV_R, p.c.ny - r0);
+            const int c0 = max(xs, 0);
+            const int c1 = min(xs + ADV_COLS, nx);
+            const uint32_t bytes = (uint32_t)(c1 - c0) * (uint32_t)sizeof(double);
+            mbar_expect_tx(&bars[st], bytes * (uint32_t)nr);
+            for (int i = 0; i < nr; ++i)
+                bulk_load(dst + i * ADV_COLS + (c0 - xs), p.Tin + (size_t)(r0 + i) * nx + c0,
+                          bytes, &bars[st]);
+        } else {
+            mbar_expect_tx(&bars[st], ADV_STAGE_DOUBLES * sizeof(double));
+            tma_load_2d(dst, map, xs, jy0 + b * ADV_R, &bars[st]);
+        }
         issued = b + 1;
     }
 
     __device__ __forceinline__ void run_task(int task) {
         const int nx = p.c.nx, ny = p.c.ny;
         const int strip = task % p.nstrips, chunk = task / p.nstrips;
+        // A warp draws tasks in increasing order, so its earlier tasks lie in
+        // lower row chunks (every cell there has a smaller flat index than
+        // every cell here: an equal peak here cannot be the first one) or in
+        // this same chunk, where it can: then equal values are examined too.
+        incl = chunk == last_chunk;
+        last_chunk = chunk;
         x0 = strip * ADV_WOUT;
         xs = x0 - ADV_KH;
         xl = xs + 4 * lane;
@@ -355,7 +405,7 @@ struct WarpStrip {
             } else {
                 st_global_v4_pred(p.Tout + (size_t)r * p.c.nx + xl, nv, owned_row && own_all);
             }
-            if constexpr (REDUCE) row_stats<T - 1>(r, nv, own_all && owned_row, true);
+            if constexpr (REDUCE) row_stats<T - 1, P>(r, nv, own_all && owned_row, true);
             fast_level<P, T + 1>(jj);
         }
     }
@@ -399,7 +449,7 @@ struct WarpStrip {
                 } else {
                     if (owned_row) store_row(r, nv);
                 }
-                if constexpr (REDUCE) row_stats<T - 1>(r, nv, owned_row && owned_lane(), !edge);
+                if constexpr (REDUCE) row_stats<T - 1, P>(r, nv, owned_row && owned_lane(), !edge);
             }
             general_level<P, T + 1>(jj);
         }
@@ -485,22 +535,38 @@ struct WarpStrip {
         const bool ol = owned_lane();
 #pragma unroll
         for (int t = 0; t < K; ++t) {
-            const double tm = rs->tmx[t][lane];
+            double tm = rs->tmx[t][lane];
+            // inclusive task: the largest double below the peak, so that
+            // equal values cross too (peaks are positive temperatures; a
+            // non-positive peak leaves the threshold where it is)
+            if (incl && tm > 0.0) tm = __longlong_as_double(__double_as_longlong(tm) - 1);
             const double a = (tm < p.c.Tm) ? tm : p.c.Tm;
             thr[t] = ol ? a : INFINITY;
         }
     }
 
-    // full: the lane's four cells are all inside the grid.
-    template <int T>
+    // full: the lane's four cells are all inside the grid.  A last-level
+    // (T == K-1) row that crosses the threshold on owned cells is staged in
+    // shared memory (box row P) for the exact pass: the last level has no
+    // register window to stage from, and a row that does not cross can hold
+    // neither a new peak nor a molten cell.
+    template <int T, int P>
     __device__ __forceinline__ void row_stats(int r, const double* nv, bool own, bool full) {
-        bool hh = hit[T];
+        bool rh = false;
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-            if (full) hh = hh | (nv[v] > thr[T]);
-            else      hh = hh | (own && xl + v < p.c.nx && nv[v] > thr[T]);
+            if (full) rh = rh | (nv[v] > thr[T]);
+            else      rh = rh | (own && xl + v < p.c.nx && nv[v] > thr[T]);
         }
-        hit[T] = hh;
+        hit[T] = hit[T] | rh;
+        if constexpr (T == K - 1) {
+            if (rh && own) {
+                double2* d = reinterpret_cast<double2*>(&rs->box[P][lane][0]);
+                d[0] = make_double2(nv[0], nv[1]);
+                d[1] = make_double2(nv[2], nv[3]);
+                kmask |= 1u << P;
+            }
+        }
     }
 
     // Copy level T's three box rows (slots of rows j-T .. j-T+2) to shared memory.
@@ -517,21 +583,23 @@ struct WarpStrip {
         }
     }
 
-    // Exact update of level t (1..K) from the box starting at row j; level-t
-    // rows come from the staging area (t < K) or from the stored field (t == K).
+    // Exact update of level t (1..K) from the box starting at row j, whose
+    // level-t rows are staged in rs->box: all three for t < K, the rows of
+    // kmask for t == K (the others crossed no threshold: every value there is
+    // at most the lane's peak so far and none is molten).
     __device__ __forceinline__ void exact_level(int t, int j) {
         const int nx = p.c.nx;
         const bool ol = owned_lane();
         double m = -INFINITY;
         for (int P = 0; P < 3; ++P) {
             const int r = j + P - t;
-            const bool cand = r >= y0 && r < y1 && ol;
+            const bool cand = r >= y0 && r < y1 && ol && (t < K || ((kmask >> P) & 1u));
             bool hot = false;
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 const bool ok = cand && xl + v < nx;
                 double x = 0.0;
-                if (ok) x = (t < K) ? rs->box[P][lane][v] : p.Tout[(size_t)r * nx + xl + v];
+                if (ok) x = rs->box[P][lane][v];
                 m = (ok && x > m) ? x : m;
                 hot |= ok && x > p.c.Tm;
             }
@@ -540,19 +608,23 @@ struct WarpStrip {
                 rs->ymx[t - 1] = max(rs->ymx[t - 1], r);
             }
         }
-        if (m > rs->tmx[t - 1][lane]) {
+        const double pk = rs->tmx[t - 1][lane];
+        if (m > pk || (incl && m == pk)) {
             long long arg = -1;
             for (int P = 0; P < 3 && arg < 0; ++P) {
                 const int r = j + P - t;
-                if (!(r >= y0 && r < y1 && ol)) continue;
+                if (!(r >= y0 && r < y1 && ol && (t < K || ((kmask >> P) & 1u)))) continue;
                 for (int v = 0; v < V; ++v) {
                     if (xl + v >= nx) break;
-                    const double x = (t < K) ? rs->box[P][lane][v] : p.Tout[(size_t)r * nx + xl + v];
+                    const double x = rs->box[P][lane][v];
                     if (x == m) { arg = (long long)r * nx + xl + v; break; }
                 }
             }
-            rs->tmx[t - 1][lane] = m;
-            rs->arg[t - 1][lane] = arg;
+            // an equal peak (inclusive task) moves only to a smaller index
+            if (m > pk || arg < rs->arg[t - 1][lane]) {
+                rs->tmx[t - 1][lane] = m;
+                rs->arg[t - 1][lane] = arg;
+            }
         }
     }
 
@@ -564,9 +636,14 @@ struct WarpStrip {
             hit[t] = false;
         }
         bits = __reduce_or_sync(0xffffffffu, bits);
-        if (bits == 0u) return;
-        for (int t = 1; t <= K; ++t) {
+        if (bits == 0u) { kmask = 0u; return; }
+        // the last level first: its rows already sit in the staging area,
+        // which the other levels then reuse
+        if ((bits >> (K - 1)) & 1u) exact_level(K, j);
+        kmask = 0u;
+        for (int t = 1; t < K; ++t) {
             if (!((bits >> (t - 1)) & 1u)) continue;
+            __syncwarp();
             switch (t) {               // stage level t's rows from its registers
                 case 1: stage_level<1>(); break;
                 case 2: stage_level<2>(); break;
@@ -575,8 +652,8 @@ struct WarpStrip {
             }
             __syncwarp();
             exact_level(t, j);
-            __syncwarp();
         }
+        __syncwarp();
     }
 };
 

@@ -133,6 +133,73 @@ int lpbf_b200_advance_noalloc(double* T_a, double* T_b, const StepConst* k,
                               const lpbf_b200_opts* opts, Partial* ring,
                               cudaStream_t stream, int* result_in_b);
 
+/* ---- Batched process map ---------------------------------------------------
+ * Replaces the reference's serial ensemble loop, one GpuStepTask graph per
+ * manifest row (src/gpu/hh_gpu_main.cpp:162-270 run_one_row/run_manifest):
+ * many independent fields of any sizes, lasers and plans advance together,
+ * `depth` time steps per launch, in one persistent kernel per launch that
+ * pulls (scenario, tile) items from a device queue.  Every scenario's field
+ * and ring are bit-identical to its own lpbf_b200_advance run.
+ *
+ * A batch is built once (lpbf_b200_batch_create: descriptors and the whole
+ * plan of every scenario go to the workspace) and run any number of times;
+ * runs are stream-ordered, allocate nothing on the device, and with
+ * use_graph != 0 replay one CUDA graph per (first step, step count, buffer
+ * parity), captured on the first such run. */
+typedef struct lpbf_b200_scenario {
+    const StepConst* k;     /* host: grid, material, dt, laser peak (x_l/y_l/q_scale unused) */
+    const lpbf_tick* plan;  /* host: the batch's n_steps Ticks (x_l, y_l, q_scale per step) */
+    double* T_a;            /* device: start field, nx*ny f64 row-major */
+    double* T_b;            /* device: the other buffer of the ping-pong pair */
+    Partial* ring;          /* device, nullable: ring[i] = Partial of plan step i */
+    int    bc;              /* 0 mirror edges, 1 fixed edges at T_edge */
+    double T_edge;          /* [K] */
+    double Tm;              /* melt threshold of the Partials [K] */
+} lpbf_b200_scenario;
+
+typedef struct lpbf_b200_batch_opts {
+    int depth;              /* time steps per launch, 1..4; 0 = 3 */
+    int ctas_per_sm;        /* CTAs per SM of the persistent grid; 0 = as many as fit */
+    int rows[4];            /* rows per task by size class (lpbf_b200_batch_size_class); 0 = 24 */
+    int staging;            /* rows into shared memory by 1 bulk row copies, 2 per-field tensor
+                               maps; 0 = automatic (maps for <= 4 fields, else bulk copies);
+                               fields with odd nx or 16-byte misalignment use direct loads */
+} lpbf_b200_batch_opts;
+
+typedef struct lpbf_b200_batch lpbf_b200_batch;   /* opaque host object */
+
+/* Size class of a grid for the per-class tile shape: 0 for max(nx, ny) < 512,
+ * 1 for < 1024, 2 for < 2048, 3 above. */
+int lpbf_b200_batch_size_class(int nx, int ny);
+/* Device workspace bytes of a batch (0 for invalid arguments). */
+size_t lpbf_b200_batch_workspace_bytes(const lpbf_b200_scenario* sc, int n_scen, int n_steps,
+                                       const lpbf_b200_batch_opts* opts);
+/* Build a batch of n_scen scenarios sharing a step count.  work: 256-byte
+ * aligned device block of lpbf_b200_batch_workspace_bytes; it belongs to the
+ * batch until lpbf_b200_batch_destroy.  Uploads the descriptors on `stream`
+ * and synchronizes it (a set-up call, not capturable).  All fields start in
+ * T_a.  *out receives a host object (host heap memory). */
+int lpbf_b200_batch_create(const lpbf_b200_scenario* sc, int n_scen, int n_steps,
+                           const lpbf_b200_batch_opts* opts, void* work, size_t work_bytes,
+                           cudaStream_t stream, lpbf_b200_batch** out);
+/* Advance every scenario through plan steps [first_step, first_step + n_steps)
+ * from the buffer that holds its current field; ring entries of those steps
+ * are written.  Asynchronous on `stream`. */
+int lpbf_b200_batch_run(lpbf_b200_batch* b, int first_step, int n_steps, int use_graph,
+                        cudaStream_t stream);
+/* 1 when the current fields are in the T_b buffers, 0 for T_a. */
+int lpbf_b200_batch_result_in_b(const lpbf_b200_batch* b);
+/* Launches that a run of n_steps issues; queue items per launch; rows per
+ * task chosen for a scenario (caller's index). */
+int lpbf_b200_batch_launches(const lpbf_b200_batch* b, int n_steps);
+int lpbf_b200_batch_tasks(const lpbf_b200_batch* b);
+int lpbf_b200_batch_scenario_rows(const lpbf_b200_batch* b, int scenario);
+/* Error word (synchronizes `stream`): bit 0 = a copy wait exceeded its time
+ * limit; the batch's counters are then undefined: destroy and re-create it. */
+int lpbf_b200_batch_read_error(const lpbf_b200_batch* b, cudaStream_t stream, unsigned int* err);
+/* Frees the host object and its graphs; the workspace is the caller's again. */
+void lpbf_b200_batch_destroy(lpbf_b200_batch* b);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
