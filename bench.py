@@ -197,6 +197,74 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def process_map_leg(args, dev):
+    """The batched process map: seeded scenarios (grid side 256..2048, power,
+    speed, spot radius, raster angle and hatch drawn per scenario) advanced
+    together through one CUDA graph of the persistent batch kernel, with
+    autotuned tiles; one scenario per size class is checked bit for bit
+    against its own single-field run, which is also timed (serial)."""
+    import torch
+    from hedgehog_lpbf_b200 import process_map as PM
+    from hedgehog_lpbf_b200.batch import Batch, autotune, opts_dict
+    from hedgehog_lpbf_b200.solver import Solver, ring_to_numpy
+    torch.cuda.empty_cache()
+    n_scen, n_steps = args.pm_scenarios, args.pm_steps
+    scs = PM.process_map(n_scen, n_steps)
+    t0 = time.time()
+    opts = autotune(scs, n_steps, cache=args.tune_cache, trial_steps=12, device=dev)
+    tune_s = time.time() - t0
+    b = Batch(scs, n_steps, opts=opts, device=dev)
+    b.capture(0, n_steps)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        e0.record()
+        b.run(0, n_steps, use_graph=True)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    cells = b.cells()
+    err = b.read_error()
+    checks, serial_ms, serial_cells = [], 0.0, 0
+    for cls in range(4):
+        idx = [i for i, sc in enumerate(scs)
+               if b.lib.lpbf_b200_batch_size_class(sc.k.nx, sc.k.ny) == cls]
+        if not idx:
+            continue
+        i = idx[0]
+        sc = scs[i]
+        s = Solver(sc.k, bc=sc.bc, T_edge=sc.T_edge, Tm=sc.Tm, device=dev, T0=sc.k.Tamb)
+        ring = s.new_ring(n_steps)
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record()
+        s.advance(sc.plan, ring)
+        f1.record()
+        torch.cuda.synchronize()
+        serial_ms += f0.elapsed_time(f1)
+        serial_cells += sc.k.nx * sc.k.ny
+        same = (torch.equal(s.field.view(torch.int64), b.field(i).view(torch.int64)) and
+                ring_to_numpy(ring).tobytes() == b.ring(i)[:n_steps].tobytes())
+        checks.append({"scenario": i, "side": sc.k.nx, "bit_identical": bool(same)})
+        del s, ring
+    out = {"value": cells * n_steps / (ms * 1e-3) / 1e9, "unit": "GCell-updates/s",
+           "workload": f"{n_scen} seeded scenarios (side 256/512/1024/2048, P 100-400 W, "
+                       f"V 0.5-2 m/s, r0 35-70 um, raster angle 0-pi, hatch 80-120 um), "
+                       f"{n_steps} steps each, FP64, uniform 300 K start",
+           "scenarios": n_scen, "steps": n_steps, "cells": cells, "ms": ms,
+           "launches": b.launches(n_steps), "tasks_per_launch": b.tasks(),
+           "tuned": opts_dict(opts), "tune_s": tune_s, "graph": True,
+           "bit_identical_to_single_runs": checks,
+           "serial_single_field": {"value": serial_cells * n_steps / (serial_ms * 1e-3) / 1e9,
+                                   "unit": "GCell-updates/s",
+                                   "scenarios": [c["scenario"] for c in checks]},
+           "clocks": clk.summary(), "error_word": err}
+    b.close()
+    return out
+
+
 def run_b200_arm(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -294,6 +362,11 @@ def run_b200_arm(args, rank, world, local_rank):
                 "bytes_per_update": 16}
         del sk, T64
 
+    pm = None
+    if args.process_map and world == 1:
+        del s
+        pm = process_map_leg(args, dev)
+
     if rank != 0:
         return
     peak, peak_src = measured_peaks()
@@ -321,6 +394,7 @@ def run_b200_arm(args, rank, world, local_rank):
                 "steps": e2e_steps},
         "gpu_launches": launches * args.steps,
         "f32k": f32k,
+        "process_map": pm,
         "clocks": clk.summary(),
         "error_word": err,
     }
@@ -342,6 +416,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-f32k", dest="f32k", action="store_false",
                     help="skip the FP32 compensated leg")
+    ap.add_argument("--no-process-map", dest="process_map", action="store_false",
+                    help="skip the batched process-map leg")
+    ap.add_argument("--pm-scenarios", type=int, default=256)
+    ap.add_argument("--pm-steps", type=int, default=5000)
+    ap.add_argument("--tune-cache", default=None,
+                    help="JSON cache of the batch autotuner (default: tune every run)")
     ap.add_argument("--side", type=int, default=N_SIDE,
                     help="grid side (smaller sides are for profiling only)")
     ap.add_argument("--iter-steps", type=int, default=STEPS_PER_ITER,

@@ -79,12 +79,20 @@ SIGNATURES = {
     "lpbf_b200_batch_create": (ctypes.c_int, [_sp, ctypes.c_int, ctypes.c_int, _bop, _vp,
                                               ctypes.c_size_t, _vp, ctypes.POINTER(_vp)]),
     "lpbf_b200_batch_run": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    "lpbf_b200_batch_capture": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "lpbf_b200_batch_result_in_b": (ctypes.c_int, [_vp]),
     "lpbf_b200_batch_launches": (ctypes.c_int, [_vp, ctypes.c_int]),
     "lpbf_b200_batch_tasks": (ctypes.c_int, [_vp]),
     "lpbf_b200_batch_scenario_rows": (ctypes.c_int, [_vp, ctypes.c_int]),
     "lpbf_b200_batch_read_error": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_uint)]),
     "lpbf_b200_batch_destroy": (None, [_vp]),
+    "lpbf_b200_batch_autotune": (ctypes.c_int, [_sp, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
+                                                ctypes.c_int, _bop]),
+    "lpbf_b200_batch_tune_key": (ctypes.c_int, [_sp, ctypes.c_int, ctypes.c_char_p,
+                                                ctypes.c_size_t]),
+    "lpbf_b200_tune_cache_get": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, _bop]),
+    "lpbf_b200_tune_cache_put": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, _bop,
+                                                ctypes.c_double]),
 }
 
 

@@ -46,6 +46,53 @@ def batch_opts(depth: int = 0, ctas_per_sm: int = 0, rows=(0, 0, 0, 0),
     return o
 
 
+def _host_array(scenarios, n_steps):
+    """lpbf_b200_scenario array with the host fields only (k, plan, edges);
+    returns it with the objects that must stay alive while it is used."""
+    arr = (_lib.Scenario * len(scenarios))()
+    keep = []
+    for i, s in enumerate(scenarios):
+        k = StepConst.from_buffer_copy(bytes(s.k))
+        plan = np.ascontiguousarray(s.plan[:n_steps], dtype=TICK_DTYPE)
+        if len(plan) < n_steps:
+            raise ValueError(f"scenario {i}: plan has {len(plan)} < {n_steps} steps")
+        keep += [k, plan]
+        arr[i].k = ctypes.pointer(k)
+        arr[i].plan = plan.ctypes.data
+        arr[i].bc = s.bc
+        arr[i].T_edge = s.T_edge
+        arr[i].Tm = s.Tm
+    return arr, keep
+
+
+def tune_key(scenarios) -> str:
+    """Cache key of a batch (GPU name, SM count, size-class histogram)."""
+    arr, _keep = _host_array(scenarios, 0)
+    buf = ctypes.create_string_buffer(512)
+    _lib.check(_lib.lib().lpbf_b200_batch_tune_key(arr, len(scenarios), buf, 512), "tune_key")
+    return buf.value.decode()
+
+
+def autotune(scenarios, n_steps: int, cache: str | None = None, trial_steps: int = 12,
+             device: torch.device | str | None = None) -> _lib.BatchOpts:
+    """Rows per size class, depth, CTAs per SM and staging for this batch,
+    from the JSON cache when it has the batch's key, else by timed trials
+    (lpbf_b200_batch_autotune; stores the result when `cache` is given)."""
+    arr, _keep = _host_array(scenarios, n_steps)
+    out = _lib.BatchOpts()
+    dev = torch.device(device) if device is not None else torch.device("cuda")
+    with torch.cuda.device(dev):
+        _lib.check(_lib.lib().lpbf_b200_batch_autotune(
+            arr, len(scenarios), n_steps, cache.encode() if cache else None,
+            min(trial_steps, n_steps), ctypes.byref(out)), "lpbf_b200_batch_autotune")
+    return out
+
+
+def opts_dict(o: _lib.BatchOpts) -> dict:
+    return {"depth": o.depth, "ctas_per_sm": o.ctas_per_sm, "staging": o.staging,
+            "rows": [o.rows[i] for i in range(4)]}
+
+
 class Batch:
     """Device state and handle of one batched process map."""
 
@@ -143,6 +190,13 @@ class Batch:
             _lib.check(self.lib.lpbf_b200_batch_run(self.handle, first_step, n, int(use_graph),
                                                     _stream_handle(stream)),
                        "lpbf_b200_batch_run")
+
+    def capture(self, first_step: int = 0, n_steps: int | None = None) -> None:
+        """Build the graph of these steps ahead of the first graph run."""
+        n = self.n_steps - first_step if n_steps is None else n_steps
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.lpbf_b200_batch_capture(self.handle, first_step, n),
+                       "lpbf_b200_batch_capture")
 
     def read_error(self) -> int:
         err = ctypes.c_uint(0)

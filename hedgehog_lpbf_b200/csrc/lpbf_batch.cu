@@ -572,11 +572,50 @@ int lpbf_b200_batch_tasks(const lpbf_b200_batch* b) {
     return b ? b->lay.ntasks : LPBF_ERR_ARG;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The cached graph of steps [first, first + n) from buffer parity `par`,
+// captured now if missing; null on failure.
+lpbf_b200_batch::Graph* batch_graph(lpbf_b200_batch* b, int first, int n, int par) {
+    for (auto& c : b->graphs)
+        if (c.exec && c.first == first && c.n == n && c.par == par) return &c;
+    if (!b->cap && cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess)
+        return nullptr;
+    lpbf_b200_batch::Graph* g = &b->graphs[b->next_graph];
+    b->next_graph ^= 1;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    *g = lpbf_b200_batch::Graph{};
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return nullptr;
+    int par_end = par;
+    const cudaError_t e1 = b->issue(first, n, par, b->cap, &par_end);
+    const cudaError_t e2 = cudaStreamEndCapture(b->cap, &graph);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return nullptr;
+    }
+    const cudaError_t e3 = cudaGraphInstantiate(&g->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e3 != cudaSuccess) { g->exec = nullptr; return nullptr; }
+    g->first = first; g->n = n; g->par = par;
+    return g;
+}
+
+bool valid_range(const lpbf_b200_batch* b, int first_step, int n_steps) {
+    return b && first_step >= 0 && n_steps >= 0 && first_step <= b->n_steps &&
+           n_steps <= b->n_steps - first_step;
+}
+
+}  // namespace
+
+extern "C" {
+
 int lpbf_b200_batch_run(lpbf_b200_batch* b, int first_step, int n_steps, int use_graph,
                         cudaStream_t stream) {
-    if (!b || first_step < 0 || n_steps < 0 || first_step > b->n_steps ||
-        n_steps > b->n_steps - first_step)
-        return LPBF_ERR_ARG;
+    if (!valid_range(b, first_step, n_steps)) return LPBF_ERR_ARG;
     if (n_steps == 0) return LPBF_OK;
     int par = b->cur;
     if (!use_graph) {
@@ -584,34 +623,17 @@ int lpbf_b200_batch_run(lpbf_b200_batch* b, int first_step, int n_steps, int use
         b->cur = par;
         return LPBF_OK;
     }
-    lpbf_b200_batch::Graph* g = nullptr;
-    for (auto& c : b->graphs)
-        if (c.exec && c.first == first_step && c.n == n_steps && c.par == par) g = &c;
-    if (!g) {
-        if (!b->cap && cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess)
-            return LPBF_ERR_CUDA;
-        g = &b->graphs[b->next_graph];
-        b->next_graph ^= 1;
-        if (g->exec) cudaGraphExecDestroy(g->exec);
-        *g = lpbf_b200_batch::Graph{};
-        cudaGraph_t graph = nullptr;
-        if (cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-            return LPBF_ERR_CUDA;
-        int par_end = par;
-        const cudaError_t e1 = b->issue(first_step, n_steps, par, b->cap, &par_end);
-        const cudaError_t e2 = cudaStreamEndCapture(b->cap, &graph);
-        if (e1 != cudaSuccess || e2 != cudaSuccess) {
-            if (graph) cudaGraphDestroy(graph);
-            return LPBF_ERR_CUDA;
-        }
-        const cudaError_t e3 = cudaGraphInstantiate(&g->exec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (e3 != cudaSuccess) { g->exec = nullptr; return LPBF_ERR_CUDA; }
-        g->first = first_step; g->n = n_steps; g->par = par;
-    }
+    lpbf_b200_batch::Graph* g = batch_graph(b, first_step, n_steps, par);
+    if (!g) return LPBF_ERR_CUDA;
     if (cudaGraphLaunch(g->exec, stream) != cudaSuccess) return LPBF_ERR_CUDA;
     b->cur = par ^ (((n_steps + b->K - 1) / b->K) & 1);
     return LPBF_OK;
+}
+
+int lpbf_b200_batch_capture(lpbf_b200_batch* b, int first_step, int n_steps) {
+    if (!valid_range(b, first_step, n_steps)) return LPBF_ERR_ARG;
+    if (n_steps == 0) return LPBF_OK;
+    return batch_graph(b, first_step, n_steps, b->cur) ? LPBF_OK : LPBF_ERR_CUDA;
 }
 
 int lpbf_b200_batch_result_in_b(const lpbf_b200_batch* b) {

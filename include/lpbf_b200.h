@@ -4,8 +4,9 @@
  *
  * Plain C (usable from C, C++, ctypes, cgo, JNI): pointers, sizes, POD
  * structs whose layouts equal the reference's StepConst / Partial / Tick.
- * Every entry point is asynchronous on `stream` unless noted, allocates
- * nothing, and returns LPBF_OK (0) or a negative status (lpbf_b200_status_string).
+ * Every entry point is asynchronous on `stream` unless noted, allocates no
+ * device memory (the autotuner excepted, as noted), and returns LPBF_OK (0)
+ * or a negative status (lpbf_b200_status_string).
  *
  * Reference interfaces these replace or extend:
  *   lpbf_b200_advance   the per-step loop of GpuStepTask::execute
@@ -187,6 +188,10 @@ int lpbf_b200_batch_create(const lpbf_b200_scenario* sc, int n_scen, int n_steps
  * are written.  Asynchronous on `stream`. */
 int lpbf_b200_batch_run(lpbf_b200_batch* b, int first_step, int n_steps, int use_graph,
                         cudaStream_t stream);
+/* Capture (without launching) the graph that lpbf_b200_batch_run with
+ * use_graph != 0 would replay for these steps from the current buffers, so
+ * that the first such run pays no capture.  Not itself capturable. */
+int lpbf_b200_batch_capture(lpbf_b200_batch* b, int first_step, int n_steps);
 /* 1 when the current fields are in the T_b buffers, 0 for T_a. */
 int lpbf_b200_batch_result_in_b(const lpbf_b200_batch* b);
 /* Launches that a run of n_steps issues; queue items per launch; rows per
@@ -199,6 +204,27 @@ int lpbf_b200_batch_scenario_rows(const lpbf_b200_batch* b, int scenario);
 int lpbf_b200_batch_read_error(const lpbf_b200_batch* b, cudaStream_t stream, unsigned int* err);
 /* Frees the host object and its graphs; the workspace is the caller's again. */
 void lpbf_b200_batch_destroy(lpbf_b200_batch* b);
+
+/* Autotuner (no reference counterpart).  Chooses rows per size class, depth,
+ * CTAs per SM and staging for this batch by timing short graph-replayed
+ * runs (trial_steps steps, <= n_steps, of the scenarios' own plans) on a
+ * subset of the scenarios (up to 2^27 cells per size class) in scratch
+ * device memory that it allocates and frees itself: a set-up call, to be
+ * made outside any stream capture, that synchronizes the device.  With
+ * cache_path non-null the result is looked up first and stored after in
+ * that JSON file, keyed by lpbf_b200_batch_tune_key.  T_a/T_b/ring of `sc`
+ * are not touched. */
+int lpbf_b200_batch_autotune(const lpbf_b200_scenario* sc, int n_scen, int n_steps,
+                             const char* cache_path, int trial_steps, lpbf_b200_batch_opts* out);
+/* Cache key of a batch: GPU name, SM count and the size-class histogram
+ * (counts rounded up to powers of two).  Host-only. */
+int lpbf_b200_batch_tune_key(const lpbf_b200_scenario* sc, int n_scen, char* buf, size_t len);
+/* The tuner's JSON cache (host-only): get returns LPBF_OK and fills *out
+ * when `key` is present, 1 when it is not, LPBF_ERR_ARG on a malformed
+ * file; put adds or replaces `key` (atomic rename). */
+int lpbf_b200_tune_cache_get(const char* path, const char* key, lpbf_b200_batch_opts* out);
+int lpbf_b200_tune_cache_put(const char* path, const char* key, const lpbf_b200_batch_opts* o,
+                             double gcells);
 
 #ifdef __cplusplus
 }  /* extern "C" */

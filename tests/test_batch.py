@@ -165,3 +165,28 @@ def test_batch_rejects_bad_arguments(gpu):
     h = ctypes.c_void_p()
     assert L.lpbf_b200_batch_create(arr, 1, 4, None, None, 0, None, ctypes.byref(h)) == -1
     assert not h.value
+
+
+def test_autotune_trials_cache_and_tuned_batch(gpu, tmp_path):
+    import json
+    import time
+
+    from hedgehog_lpbf_b200.batch import Batch, autotune, opts_dict, tune_key
+    n = 12
+    scs = _mixed(n, [(256, 256, 0), (600, 520, 0), (1100, 1030, 1), (300, 2050, 0)], seed=11)
+    cache = str(tmp_path / "tune.json")
+    o1 = autotune(scs, n, cache=cache, trial_steps=6)
+    d1 = opts_dict(o1)
+    assert d1["depth"] in (2, 3, 4) and d1["staging"] in (1, 2)
+    assert all(r in (12, 24, 48, 96, 192) for r in d1["rows"])
+    doc = json.load(open(cache))
+    assert tune_key(scs) in doc["entries"] and doc["entries"][tune_key(scs)]["gcells"] > 0
+    t0 = time.time()
+    o2 = autotune(scs, n, cache=cache, trial_steps=6)       # from the cache
+    assert opts_dict(o2) == d1 and time.time() - t0 < 1.0
+    refs = [_single(sc, n) for sc in scs]
+    b = Batch(scs, n, opts=o1, device="cuda:0")
+    b.capture(0, n)
+    b.run(0, n, use_graph=True)
+    _assert_same(b, scs, n, refs)
+    b.close()

@@ -79,3 +79,44 @@ def test_batch_size_classes_and_workspace_bytes():
     assert small < b1                             # fewer tasks, fewer partials
     assert L.lpbf_b200_batch_workspace_bytes(arr, len(scs), 10,
                                              ctypes.byref(batch_opts(depth=9))) == 0
+
+
+def test_tune_cache_round_trip(tmp_path):
+    from hedgehog_lpbf_b200.batch import batch_opts, opts_dict
+    L = _lib.lib()
+    path = str(tmp_path / "tune.json").encode()
+    out = _lib.BatchOpts()
+    assert L.lpbf_b200_tune_cache_get(path, b"gpu|sm148|classes 64,64,64,64", ctypes.byref(out)) == 1
+    o1 = batch_opts(depth=2, ctas_per_sm=2, rows=(24, 48, 96, 192), staging=1)
+    o2 = batch_opts(depth=3, rows=(12, 12, 24, 24), staging=2)
+    assert L.lpbf_b200_tune_cache_put(path, b"k1", ctypes.byref(o1), 241.5) == 0
+    assert L.lpbf_b200_tune_cache_put(path, b'k "2"', ctypes.byref(o2), 300.0) == 0
+    assert L.lpbf_b200_tune_cache_get(path, b"k1", ctypes.byref(out)) == 0
+    assert opts_dict(out) == opts_dict(o1)
+    assert L.lpbf_b200_tune_cache_get(path, b'k "2"', ctypes.byref(out)) == 0
+    assert opts_dict(out) == opts_dict(o2)
+    import json
+    doc = json.load(open(path.decode()))          # the file is plain JSON
+    assert doc["version"] == 1 and doc["entries"]["k1"]["rows"] == [24, 48, 96, 192]
+    assert doc["entries"]["k1"]["gcells"] == 241.5
+    # replacing a key keeps the others
+    assert L.lpbf_b200_tune_cache_put(path, b"k1", ctypes.byref(o2), 1.0) == 0
+    assert L.lpbf_b200_tune_cache_get(path, b"k1", ctypes.byref(out)) == 0
+    assert opts_dict(out) == opts_dict(o2)
+    assert L.lpbf_b200_tune_cache_get(path, b'k "2"', ctypes.byref(out)) == 0
+    # a malformed file is an error for get and is rewritten by put
+    open(path.decode(), "w").write("{not json")
+    assert L.lpbf_b200_tune_cache_get(path, b"k1", ctypes.byref(out)) == -1
+    assert L.lpbf_b200_tune_cache_put(path, b"k3", ctypes.byref(o1), 2.0) == 0
+    assert L.lpbf_b200_tune_cache_get(path, b"k3", ctypes.byref(out)) == 0
+
+
+def test_tune_key_is_the_size_class_histogram():
+    from hedgehog_lpbf_b200.batch import tune_key
+    scs = PM.process_map(40, 2)
+    key = tune_key(scs)
+    counts = [0, 0, 0, 0]
+    for s in scs:
+        counts[_lib.lib().lpbf_b200_batch_size_class(s.k.nx, s.k.ny)] += 1
+    pow2 = [0 if c == 0 else 1 << (c - 1).bit_length() for c in counts]
+    assert key.endswith("classes " + ",".join(map(str, pow2)))
