@@ -41,6 +41,13 @@ class BatchOpts(ctypes.Structure):
                 ("rows", ctypes.c_int * 4), ("staging", ctypes.c_int)]
 
 
+class SgConvArgs(ctypes.Structure):
+    """lpbf_b200_sg_conv_args (include/lpbf_b200.h)."""
+    _fields_ = [("x", _vp), ("w", _vp), ("bias", _vp), ("pre_in", _vp), ("pre_out", _vp),
+                ("out", _vp), ("batch", ctypes.c_int), ("height", ctypes.c_int),
+                ("width", ctypes.c_int), ("err", _vp)]
+
+
 _sp = ctypes.POINTER(Scenario)
 _bop = ctypes.POINTER(BatchOpts)
 
@@ -93,6 +100,8 @@ SIGNATURES = {
     "lpbf_b200_tune_cache_get": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, _bop]),
     "lpbf_b200_tune_cache_put": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, _bop,
                                                 ctypes.c_double]),
+    "lpbf_b200_sg_conv": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(SgConvArgs), _vp]),
+    "lpbf_b200_sg_gemm_bt": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
 }
 
 

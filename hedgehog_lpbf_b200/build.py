@@ -25,6 +25,22 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
               "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 
 
+def cutlass_include() -> str:
+    """CUTLASS/CuTe headers (sm100 UMMA atoms) vendored with the image's
+    flashinfer (or tilelang) package; the tensor-core kernels need them."""
+    import importlib.util
+    for pkg, sub in (("flashinfer", ("data", "cutlass", "include")),
+                     ("tilelang", ("3rdparty", "cutlass", "include"))):
+        spec = importlib.util.find_spec(pkg)
+        if spec is None or not spec.submodule_search_locations:
+            continue
+        for loc in spec.submodule_search_locations:
+            d = os.path.join(loc, *sub)
+            if os.path.exists(os.path.join(d, "cute", "atom", "mma_traits_sm100.hpp")):
+                return d
+    raise RuntimeError("CUTLASS/CuTe headers with sm100 support not found")
+
+
 def sources() -> list[str]:
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
@@ -53,7 +69,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
         return LIB
     objdir = os.path.join(PKG, "_build")
     os.makedirs(objdir, exist_ok=True)
-    inc = ["-I" + INCLUDE, "-I" + CSRC]
+    inc = ["-I" + INCLUDE, "-I" + CSRC, "-I" + cutlass_include()]
     objs, procs = [], []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")

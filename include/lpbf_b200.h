@@ -226,6 +226,45 @@ int lpbf_b200_tune_cache_get(const char* path, const char* key, lpbf_b200_batch_
 int lpbf_b200_tune_cache_put(const char* path, const char* key, const lpbf_b200_batch_opts* o,
                              double gcells);
 
+/* ---- Learned super-stepper: convolution layers on tcgen05 tensor cores ------
+ * No reference counterpart (the reference has no learned component).  Each
+ * call runs one 3x3 convolution layer (zero padding) over `batch` images of
+ * height x width pixels as an implicit GEMM on the tensor cores: bf16
+ * operands, fp32 accumulation in tensor memory.  Activations are NHWC bf16;
+ * weights are packed [N][K] bf16 with K = 9 taps x C_in (tap-major, taps in
+ * row-major 3x3 order, (dy, dx) = (tap / 3 - 1, tap % 3 - 1)), padded with
+ * zeros to 64 when 9 x C_in < 64; N = 32, or 16 for the output layer (row 0
+ * real, the rest zero).
+ *   LPBF_SG_FWD_IN     C_in 4 -> 32, out = gelu(conv + bias), pre_out = conv + bias
+ *   LPBF_SG_FWD_HIDDEN C_in 32 -> 32, same epilogue
+ *   LPBF_SG_FWD_OUT    C_in 32 -> 1 (N = 16), out (fp32) = conv[0] + bias[0]
+ *   LPBF_SG_DX_OUT     C_in 1 -> 32, out = conv * gelu'(pre_in)
+ *   LPBF_SG_DX_HIDDEN  C_in 32 -> 32, out = conv * gelu'(pre_in)
+ * The DX kinds give the gradient of the previous layer's pre-activation
+ * when x is this layer's pre-activation gradient and the weights are packed
+ * transposed with the taps flipped.  err (nullable): bit 0 set when a
+ * tensor-core completion wait ran out of time. */
+enum {
+    LPBF_SG_FWD_IN = 0, LPBF_SG_FWD_HIDDEN = 1, LPBF_SG_FWD_OUT = 2,
+    LPBF_SG_DX_OUT = 3, LPBF_SG_DX_HIDDEN = 4
+};
+typedef struct lpbf_b200_sg_conv_args {
+    const void*  x;        /* input activations, NHWC bf16 */
+    const void*  w;        /* packed weights, bf16 [N][K] */
+    const float* bias;     /* [N] fp32 (forward kinds) */
+    const void*  pre_in;   /* DX kinds: pre-activation of the target layer, bf16 [P][32] */
+    void*        pre_out;  /* FWD_IN/FWD_HIDDEN: pre-activation out, bf16 [P][32], nullable */
+    void*        out;      /* bf16 [P][32], or fp32 [P] for FWD_OUT */
+    int batch, height, width;
+    unsigned int* err;
+} lpbf_b200_sg_conv_args;
+int lpbf_b200_sg_conv(int kind, const lpbf_b200_sg_conv_args* args, cudaStream_t stream);
+/* C[128 x n] (fp32, row-major) = A[128 x k] . B[n x k]^T, bf16 row-major
+ * operands, on the tensor cores (one CTA; n = 16 or 32, k = 288): the
+ * matrix core of the layers alone, for diagnostics. */
+int lpbf_b200_sg_gemm_bt(const void* A, const void* B, float* C, int n, int k,
+                         unsigned int* err, cudaStream_t stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

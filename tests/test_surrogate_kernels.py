@@ -1,0 +1,129 @@
+# SPDX-License-Identifier: 0BSD
+"""Tensor-core layers of the learned super-stepper (lpbf_b200_sg_conv,
+lpbf_b200_sg_gemm_bt) against the FP64 numpy restatement in
+oracle/surrogate_ref.py, on the same bf16-rounded operands.  Tolerance: the
+fp32-accumulated result is rounded to bf16 on output (relative step 2^-8),
+so outputs agree within 1e-2 relative to the largest output magnitude."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import surrogate_ref as R
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16(a):
+    import torch
+    return torch.tensor(np.asarray(a, dtype=np.float32)).to(torch.bfloat16)
+
+
+def _np(t):
+    import torch
+    return t.float().cpu().numpy().astype(np.float64) if t.dtype == torch.bfloat16 \
+        else t.cpu().numpy().astype(np.float64)
+
+
+def _conv(kind, x, wp, bias=None, pre_in=None, want_pre=False, out_fp32=False):
+    import torch
+    from hedgehog_lpbf_b200 import _lib
+    L = _lib.lib()
+    dev = torch.device("cuda:0")
+    B, H, W = x.shape[:3]
+    xd = x.to(dev).contiguous()
+    wd = wp.to(dev).contiguous()
+    bd = torch.tensor(bias, dtype=torch.float32, device=dev) if bias is not None else None
+    pid = pre_in.to(dev).contiguous() if pre_in is not None else None
+    if out_fp32:
+        out = torch.zeros((B, H, W), dtype=torch.float32, device=dev)
+    else:
+        out = torch.zeros((B, H, W, 32), dtype=torch.bfloat16, device=dev)
+    pre = torch.zeros((B, H, W, 32), dtype=torch.bfloat16, device=dev) if want_pre else None
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    a = _lib.SgConvArgs(x=xd.data_ptr(), w=wd.data_ptr(), bias=bd.data_ptr() if bd is not None else None,
+                        pre_in=pid.data_ptr() if pid is not None else None,
+                        pre_out=pre.data_ptr() if pre is not None else None, out=out.data_ptr(),
+                        batch=B, height=H, width=W, err=err.data_ptr())
+    st = L.lpbf_b200_sg_conv(kind, ctypes.byref(a), torch.cuda.current_stream().cuda_stream)
+    assert st == 0, L.lpbf_b200_status_string(st)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    return out, pre
+
+
+def _close(got, ref, rtol=1e-2):
+    scale = max(np.max(np.abs(ref)), 1e-6)
+    assert np.max(np.abs(got - ref)) <= rtol * scale, (np.max(np.abs(got - ref)), scale)
+
+
+def test_tile_product_on_tensor_cores(gpu):
+    import torch
+    from hedgehog_lpbf_b200 import _lib
+    L = _lib.lib()
+    rng = np.random.default_rng(0)
+    for n in (32, 16):
+        A = _bf16(rng.normal(size=(128, 288)))
+        B = _bf16(rng.normal(size=(n, 288)))
+        C = torch.zeros((128, n), dtype=torch.float32, device="cuda:0")
+        err = torch.zeros(1, dtype=torch.int32, device="cuda:0")
+        Ad, Bd = A.cuda(), B.cuda()
+        assert L.lpbf_b200_sg_gemm_bt(Ad.data_ptr(), Bd.data_ptr(), C.data_ptr(), n, 288,
+                                      err.data_ptr(), None) == 0
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0
+        ref = _np(A) @ _np(B).T
+        assert np.max(np.abs(_np(C) - ref)) <= 1e-4 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("B,H,W", [(1, 3, 128), (2, 5, 200), (1, 2, 300)])
+def test_forward_layers(gpu, B, H, W):
+    rng = np.random.default_rng(1)
+    ps = R.init_params(3)
+    x4 = _bf16(rng.normal(size=(B, H, W, 4)))
+    # input layer 4 -> 32
+    w, b = ps[0]
+    b = rng.normal(size=32) * 0.1
+    act, pre = _conv(0, x4, _bf16(R.pack(w, k_pad=64)), bias=b, want_pre=True)
+    ref_pre = R.conv3x3(_np(x4), _np(_bf16(w.reshape(32, -1))).reshape(w.shape), b)
+    _close(_np(pre), ref_pre)
+    _close(_np(act), R.gelu(_np(pre)))
+    # hidden 32 -> 32 on the (bf16) activations
+    w, _ = ps[1]
+    wq = _np(_bf16(w.reshape(32, -1))).reshape(w.shape)
+    act2, pre2 = _conv(1, act, _bf16(R.pack(w)), bias=b, want_pre=True)
+    _close(_np(pre2), R.conv3x3(_np(act), wq, b))
+    # output 32 -> 1
+    w, _ = ps[4]
+    wq = _np(_bf16(w.reshape(1, -1))).reshape(w.shape)
+    y, _ = _conv(2, act2, _bf16(R.pack(w, n_pad=16)), bias=np.array([0.25]), out_fp32=True)
+    _close(_np(y), R.conv3x3(_np(act2), wq, np.array([0.25]))[..., 0], rtol=2e-3)
+
+
+def test_input_gradient_layers(gpu):
+    rng = np.random.default_rng(2)
+    B, H, W = 2, 4, 170
+    ps = R.init_params(5)
+    pre_prev = _bf16(rng.normal(size=(B, H, W, 32)))
+    # output layer: upstream gradient has one channel
+    g5 = _bf16(rng.normal(size=(B, H, W, 1)))
+    w5 = ps[4][0]
+    wt = R.flip_transpose(w5)                      # [32, 9, 1]
+    out, _ = _conv(3, g5, _bf16(R.pack(wt, k_pad=64)), pre_in=pre_prev)
+    wq = _np(_bf16(wt.reshape(32, -1))).reshape(wt.shape)
+    ref = R.conv3x3(_np(g5), wq) * R.gelu_grad(_np(pre_prev))
+    _close(_np(out), ref)
+    # hidden layer
+    g = _bf16(rng.normal(size=(B, H, W, 32)))
+    w = ps[2][0]
+    wt = R.flip_transpose(w)
+    out, _ = _conv(4, g, _bf16(R.pack(wt)), pre_in=pre_prev)
+    wq = _np(_bf16(wt.reshape(32, -1))).reshape(wt.shape)
+    ref = R.conv3x3(_np(g), wq) * R.gelu_grad(_np(pre_prev))
+    _close(_np(out), ref)
+    # the flipped-transposed weights are the adjoint of the forward conv
+    x = rng.normal(size=(1, 3, 7, 32))
+    gg = rng.normal(size=(1, 3, 7, 32))
+    lhs = np.sum(R.conv3x3(x, w) * gg)
+    rhs = np.sum(x * R.conv3x3_input_grad(gg, w))
+    assert abs(lhs - rhs) <= 1e-9 * abs(lhs)
