@@ -48,6 +48,12 @@ class SgConvArgs(ctypes.Structure):
                 ("width", ctypes.c_int), ("err", _vp)]
 
 
+class SgHyper(ctypes.Structure):
+    """lpbf_b200_sg_hyper (include/lpbf_b200.h)."""
+    _fields_ = [("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
+                ("eps", ctypes.c_float), ("weight_decay", ctypes.c_float), ("step", ctypes.c_int)]
+
+
 _sp = ctypes.POINTER(Scenario)
 _bop = ctypes.POINTER(BatchOpts)
 
@@ -102,6 +108,23 @@ SIGNATURES = {
                                                 ctypes.c_double]),
     "lpbf_b200_sg_conv": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(SgConvArgs), _vp]),
     "lpbf_b200_sg_gemm_bt": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "lpbf_b200_sg_param_count": (ctypes.c_int, []),
+    "lpbf_b200_sg_net_bytes": (ctypes.c_size_t, []),
+    "lpbf_b200_sg_work_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_int]),
+    "lpbf_b200_sg_net_set": (ctypes.c_int, [_vp, _vp, _vp]),
+    "lpbf_b200_sg_net_get": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "lpbf_b200_sg_forward": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, _vp, ctypes.c_size_t, _vp, _vp]),
+    "lpbf_b200_sg_gradients": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, _vp, ctypes.c_size_t, _vp, _vp, _vp]),
+    "lpbf_b200_sg_adamw": (ctypes.c_int, [_vp, ctypes.POINTER(SgHyper), _vp]),
+    "lpbf_b200_sg_train_step": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.POINTER(SgHyper), _vp,
+                                               ctypes.c_size_t, _vp, _vp, _vp]),
+    "lpbf_b200_sg_features": (ctypes.c_int, [_vp, ctypes.POINTER(StepConst), _vp, _vp, _vp]),
+    "lpbf_b200_sg_apply": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _vp]),
+    "lpbf_b200_sg_target": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_longlong, _vp]),
 }
 
 

@@ -60,8 +60,10 @@ struct TileMma {
     }
 
     // Issue the whole K reduction into tensor memory at `tmem` and commit
-    // to `bar`.  Called by one full warp (the atom elects one thread).
-    __device__ static void issue(bf16* sA, bf16* sB, uint32_t tmem, uint64_t* bar) {
+    // to `bar`; `accumulate` adds to the accumulator instead of starting it.
+    // Called by one full warp (the atom elects one thread).
+    __device__ static void issue(bf16* sA, bf16* sB, uint32_t tmem, uint64_t* bar,
+                                 bool accumulate = false) {
         using namespace cute;
         auto tiled = make_tiled_mma(Op{});
         Tensor tA = make_tensor(make_smem_ptr(sA), LayA{});
@@ -75,7 +77,7 @@ struct TileMma {
                                 make_shape(Int<M>{}, Int<N>{}), LayoutRight{});
         Tensor tCtAcc = thr.make_fragment_C(thr.partition_C(gC));
         tCtAcc.data() = tmem;
-        tiled.accumulate_ = UMMA::ScaleOut::Zero;
+        tiled.accumulate_ = accumulate ? UMMA::ScaleOut::One : UMMA::ScaleOut::Zero;
         CUTE_UNROLL
         for (int k = 0; k < size<2>(tCrA); ++k) {
             gemm(tiled, tCrA(_, _, k), tCrB(_, _, k), tCtAcc);

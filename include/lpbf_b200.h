@@ -259,6 +259,61 @@ typedef struct lpbf_b200_sg_conv_args {
     unsigned int* err;
 } lpbf_b200_sg_conv_args;
 int lpbf_b200_sg_conv(int kind, const lpbf_b200_sg_conv_args* args, cudaStream_t stream);
+/* ---- The network: parameters, training, features ----------------------------
+ * 5 layers (4 -> 32 -> 32 -> 32 -> 32 -> 1 channels, GELU after the first
+ * four).  Inputs per pixel, bf16 NHWC: (T - T_amb) / LPBF_SG_T_SCALE, the
+ * Gaussian source summed over the next LPBF_SG_STEPS steps / LPBF_SG_S_SCALE,
+ * and the pixel's x and y offset from the laser at the middle of those steps
+ * / LPBF_SG_POS_SCALE (clamped to +-8).  Output (fp32): the field's change
+ * over those steps / LPBF_SG_DT_SCALE.
+ * The network blob (lpbf_b200_sg_net_bytes, caller-allocated device memory)
+ * holds fp32 parameters (LPBF_SG_PARAMS = lpbf_b200_sg_param_count(), layer
+ * by layer W[c_out][9][c_in] then b[c_out]), their gradients, the AdamW
+ * moments and the packed bf16 weights. */
+#define LPBF_SG_STEPS 16
+#define LPBF_SG_T_SCALE 1000.0
+#define LPBF_SG_S_SCALE 1000.0
+#define LPBF_SG_DT_SCALE 100.0
+#define LPBF_SG_POS_SCALE 100e-6
+typedef struct lpbf_b200_sg_hyper {
+    float lr, beta1, beta2, eps, weight_decay;
+    int step;                 /* 1-based AdamW step (bias correction) */
+} lpbf_b200_sg_hyper;
+int    lpbf_b200_sg_param_count(void);
+size_t lpbf_b200_sg_net_bytes(void);
+/* Activation workspace for batch x height x width pixels (train != 0: the
+ * training step, which keeps every layer's activations and gradients). */
+size_t lpbf_b200_sg_work_bytes(int batch, int height, int width, int train);
+/* Set the parameters from fp32 `params` (host or device), zero the AdamW
+ * moments and gradients, pack the bf16 weights. */
+int lpbf_b200_sg_net_set(void* net, const float* params, cudaStream_t stream);
+/* Copy parameters and/or gradients (fp32, host or device; nullable). */
+int lpbf_b200_sg_net_get(const void* net, float* params, float* grads, cudaStream_t stream);
+/* y (fp32, batch x height x width) from inputs x4 (bf16 [P][4]). */
+int lpbf_b200_sg_forward(const void* net, const void* x4, float* y, int batch, int height,
+                         int width, void* work, size_t work_bytes, unsigned int* err,
+                         cudaStream_t stream);
+/* Mean squared error against `target` (fp32 [P]) into *loss (device,
+ * nullable) and its gradients into the blob's gradient section. */
+int lpbf_b200_sg_gradients(void* net, const void* x4, const float* target, int batch, int height,
+                           int width, void* work, size_t work_bytes, float* loss,
+                           unsigned int* err, cudaStream_t stream);
+/* One AdamW step (decoupled weight decay) from the stored gradients; repacks
+ * the bf16 weights. */
+int lpbf_b200_sg_adamw(void* net, const lpbf_b200_sg_hyper* h, cudaStream_t stream);
+/* gradients + adamw. */
+int lpbf_b200_sg_train_step(void* net, const void* x4, const float* target, int batch, int height,
+                            int width, const lpbf_b200_sg_hyper* h, void* work, size_t work_bytes,
+                            float* loss, unsigned int* err, cudaStream_t stream);
+/* Network inputs for the field T (device, nx x ny f64) before plan[0 ..
+ * LPBF_SG_STEPS) (host Ticks) into x4 (device bf16 [ny][nx][4]). */
+int lpbf_b200_sg_features(const double* T, const StepConst* k, const lpbf_tick* plan,
+                          void* x4, cudaStream_t stream);
+/* T += y * LPBF_SG_DT_SCALE (one super-step), and the training target
+ * t = (T1 - T0) / LPBF_SG_DT_SCALE. */
+int lpbf_b200_sg_apply(double* T, const float* y, long long n, cudaStream_t stream);
+int lpbf_b200_sg_target(const double* T0, const double* T1, float* t, long long n,
+                        cudaStream_t stream);
 /* C[128 x n] (fp32, row-major) = A[128 x k] . B[n x k]^T, bf16 row-major
  * operands, on the tensor cores (one CTA; n = 16 or 32, k = 288): the
  * matrix core of the layers alone, for diagnostics. */

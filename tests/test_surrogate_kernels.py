@@ -127,3 +127,94 @@ def test_input_gradient_layers(gpu):
     lhs = np.sum(R.conv3x3(x, w) * gg)
     rhs = np.sum(x * R.conv3x3_input_grad(gg, w))
     assert abs(lhs - rhs) <= 1e-9 * abs(lhs)
+
+
+def _rand_net(seed, out_std=0.3):
+    ps = R.init_params(seed)
+    rng = np.random.default_rng(seed + 100)
+    ps = [(w, rng.normal(0, 0.05, b.shape)) for w, b in ps]
+    w5, b5 = ps[4]
+    ps[4] = (w5 * out_std / 0.1 * 10, b5)
+    return ps
+
+
+def _bf16_params(ps):
+    return [(_np(_bf16(w.reshape(w.shape[0], -1))).reshape(w.shape), b) for w, b in ps]
+
+
+def test_weight_gradients_match_fp64_backward(gpu):
+    """Gradient check: the GPU's loss and per-layer gradients (bf16 operands,
+    fp32 accumulation) against the FP64 backward pass of oracle/surrogate_ref
+    on the same bf16-rounded inputs and weights."""
+    import torch
+    from hedgehog_lpbf_b200.surrogate import Net, unflatten
+    rng = np.random.default_rng(7)
+    B, H, W = 2, 6, 150
+    ps = _rand_net(3)
+    x4 = _bf16(rng.normal(size=(B, H, W, 4)))
+    tgt = rng.normal(size=(B, H, W)).astype(np.float32)
+    net = Net(ps, device="cuda:0")
+    loss = net.gradients(x4.cuda(), torch.tensor(tgt, device="cuda:0"))
+    torch.cuda.synchronize()
+    assert net.error_word() == 0
+    g_gpu = unflatten(net.grads_vector())
+    loss_ref, g_ref = R.loss_and_grads(_bf16_params(ps), _np(x4), tgt.astype(np.float64))
+    assert abs(float(loss.item()) - loss_ref) <= 1e-2 * loss_ref
+    for li in range(5):
+        for part in (0, 1):
+            a, b = g_gpu[li][part].ravel(), g_ref[li][part].ravel()
+            rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+            cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
+            assert rel < 3e-2 and cos > 0.999, (li, part, rel, cos)
+
+
+def test_adamw_step_matches_reference(gpu):
+    import torch
+    from hedgehog_lpbf_b200.surrogate import Net
+    rng = np.random.default_rng(8)
+    ps = _rand_net(4)
+    x4 = _bf16(rng.normal(size=(1, 4, 130, 4)))
+    tgt = torch.tensor(rng.normal(size=(1, 4, 130)).astype(np.float32), device="cuda:0")
+    net = Net(ps, device="cuda:0")
+    p0 = net.params_vector().astype(np.float64)
+    net.train_step(x4.cuda(), tgt, lr=1e-3, weight_decay=0.01)
+    torch.cuda.synchronize()
+    g = net.grads_vector().astype(np.float64)
+    p1 = net.params_vector().astype(np.float64)
+    ref, _, _ = R.adamw(p0, g, np.zeros_like(g), np.zeros_like(g), 1, lr=1e-3, wd=0.01)
+    assert np.max(np.abs(p1 - ref)) <= 1e-6 * max(1.0, np.max(np.abs(ref)))
+    # a second step moves on from the stored moments
+    net.train_step(x4.cuda(), tgt, lr=1e-3, weight_decay=0.01)
+    torch.cuda.synchronize()
+    assert not np.array_equal(net.params_vector(), p1.astype(np.float32))
+
+
+def test_features_and_apply(gpu):
+    import torch
+    from hedgehog_lpbf_b200 import params as P
+    from hedgehog_lpbf_b200 import plan as PL
+    from hedgehog_lpbf_b200.surrogate import features, apply, target, STEPS
+    mat, pr = P.benchmark_material_process()
+    dom = P.square_domain(200)
+    k = P.make_const(mat, pr, dom, P.dt_fraction(mat, dom))
+    plan = PL.raster_for_steps(dom, k.dt, 64, V=1.0, hatch=100e-6, n_tracks=2)
+    rng = np.random.default_rng(3)
+    T = 300.0 + rng.uniform(0, 1500, size=(200, 200))
+    Td = torch.tensor(T, device="cuda:0")
+    x4 = features(Td, k, plan).float().cpu().numpy()
+    yy, xx = np.meshgrid(np.arange(200) * k.dy, np.arange(200) * k.dx, indexing="ij")
+    S = np.zeros_like(T)
+    for s in range(STEPS):
+        cs = k.dt * (plan["q_scale"][s] * k.peak_S) / (k.rho_cp * k.h)
+        r2 = (xx - plan["x_l"][s]) ** 2 + (yy - plan["y_l"][s]) ** 2
+        S += cs * np.exp(-2.0 * r2 * k.inv_r0_sq)
+    ref = np.stack([(T - k.Tamb) / 1000.0, S / 1000.0,
+                    np.clip((xx - plan["x_l"][8]) / 100e-6, -8, 8),
+                    np.clip((yy - plan["y_l"][8]) / 100e-6, -8, 8)], axis=-1)
+    assert np.max(np.abs(x4 - ref)) <= 1e-2 * np.max(np.abs(ref))
+    y = torch.tensor(rng.normal(size=(200, 200)).astype(np.float32), device="cuda:0")
+    T1 = Td.clone()
+    apply(T1, y)
+    assert np.allclose(T1.cpu().numpy(), T + 100.0 * y.cpu().numpy().astype(np.float64))
+    t = target(Td, T1).cpu().numpy()
+    assert np.allclose(t, y.cpu().numpy(), rtol=1e-5, atol=1e-5)
