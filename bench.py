@@ -265,6 +265,98 @@ def process_map_leg(args, dev):
     return out
 
 
+FLOP_PER_PIXEL = 2 * 9 * (4 * 32 + 3 * 32 * 32 + 32 * 1)   # one forward of the super-stepper
+
+
+def superstep_leg(args, dev):
+    """The learned super-stepper (committed weights trained by this library's
+    own tcgen05 kernels): forward throughput on the 4096^2 field, training
+    step throughput (batch 32 of 256^2 patches), and the hybrid run with the
+    FP64 judge and rollback on the 4096^2 raster (20 tracks, 100 um hatch,
+    1 m/s) over a prefix of its 200,000 steps, against plain FP64 on the
+    same prefix."""
+    import torch
+    from hedgehog_lpbf_b200 import params as P
+    from hedgehog_lpbf_b200 import plan as PL
+    from hedgehog_lpbf_b200.solver import Solver
+    from hedgehog_lpbf_b200.superstep import WEIGHTS, load, run_hybrid
+    from hedgehog_lpbf_b200.surrogate import STEPS, Net, features, init_params
+    torch.cuda.empty_cache()
+    if os.path.exists(WEIGHTS):
+        net, rec = load(WEIGHTS, device=dev)
+    else:
+        net, rec = Net(init_params(0), device=dev), None
+    mat, pr = P.benchmark_material_process()
+    dom = P.square_domain(4096)
+    dt = P.dt_fraction(mat, dom)
+    k = P.make_const(mat, pr, dom, dt)
+    plan = PL.raster_for_steps(dom, dt, 200000, V=1.0, hatch=100e-6, n_tracks=20)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        ev[0].record()
+        for _ in range(reps):
+            fn()
+        ev[1].record()
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / reps
+
+    T = torch.full((4096, 4096), 300.0, dtype=torch.float64, device=dev)
+    x4 = features(T, k, plan[:STEPS])[None]
+    y = torch.empty((1, 4096, 4096), dtype=torch.float32, device=dev)
+    fwd_ms = timed(lambda: net.forward(x4, y), 5)
+    px = 4096 * 4096
+    del x4, y
+    tnet = Net(init_params(1), device=dev)
+    xb = torch.randn((32, 256, 256, 4), device=dev).to(torch.bfloat16)
+    tb = torch.randn((32, 256, 256), dtype=torch.float32, device=dev)
+    tr_ms = timed(lambda: tnet.train_step(xb, tb), 10)
+    del tnet, xb, tb
+    torch.cuda.empty_cache()
+    # hybrid vs plain FP64 on a prefix of the 4096^2 raster
+    n = args.ss_steps
+    T0 = np.full(px, 300.0)
+    Th, hyb = run_hybrid(net, k, plan, T0, n, judge_every=8, tol_K=5.0, area_tol=0.02,
+                         Tm=mat.Tm, device=dev)
+    s = Solver(k, Tm=mat.Tm, device=dev, depth=3)
+    s.set_field(300.0)
+    torch.cuda.synchronize()
+    ev[0].record()
+    s.advance(plan[:hyb["steps"]])
+    ev[1].record()
+    torch.cuda.synchronize()
+    plain_ms = ev[0].elapsed_time(ev[1])
+    Tp = s.field
+    melt_p = int((Tp > mat.Tm).sum().item())
+    melt_h = int((Th > mat.Tm).sum().item())
+    out = {
+        "network": "5 x conv3x3 (4-32-32-32-32-1), GELU, bf16 on tcgen05, fp32 accumulation",
+        "weights": "committed" if rec else "untrained (no weights file)",
+        "forward_4096sq": {"ms": fwd_ms,
+                           "gcell_updates_equiv": px * STEPS / (fwd_ms * 1e-3) / 1e9,
+                           "tflops": FLOP_PER_PIXEL * px / (fwd_ms * 1e-3) / 1e12},
+        "train_step_32x256sq": {"ms": tr_ms,
+                                "tflops": 3 * FLOP_PER_PIXEL * 32 * 256 * 256 / (tr_ms * 1e-3) / 1e12},
+        "hybrid_4096sq": {"steps": hyb["steps"], "hybrid_ms": hyb["gpu_ms"], "plain_fp64_ms": plain_ms,
+                          "speedup_vs_plain": plain_ms / hyb["gpu_ms"],
+                          "max_abs_err_vs_fp64_K": float((Th - Tp).abs().max().item()),
+                          "melt_area_err": abs(melt_h - melt_p) / max(melt_p, 1),
+                          "judged": hyb["judged"], "rolled_back": hyb["rolled_back"],
+                          "worst_window_K": hyb["worst_K"]},
+        "heldout": rec.get("heldout_trained") if rec else None,
+    }
+    peak = None
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        with open(pk) as f:
+            peak = json.load(f).get("bf16_tflops")
+    if peak:
+        out["forward_4096sq"]["frac_of_measured_bf16"] = out["forward_4096sq"]["tflops"] / peak
+    return out
+
+
 def run_b200_arm(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -366,6 +458,9 @@ def run_b200_arm(args, rank, world, local_rank):
     if args.process_map and world == 1:
         del s
         pm = process_map_leg(args, dev)
+    ss = None
+    if args.superstep and world == 1:
+        ss = superstep_leg(args, dev)
 
     if rank != 0:
         return
@@ -395,6 +490,7 @@ def run_b200_arm(args, rank, world, local_rank):
         "gpu_launches": launches * args.steps,
         "f32k": f32k,
         "process_map": pm,
+        "superstep": ss,
         "clocks": clk.summary(),
         "error_word": err,
     }
@@ -420,6 +516,10 @@ def main():
                     help="skip the batched process-map leg")
     ap.add_argument("--pm-scenarios", type=int, default=256)
     ap.add_argument("--pm-steps", type=int, default=5000)
+    ap.add_argument("--no-superstep", dest="superstep", action="store_false",
+                    help="skip the learned super-stepper leg")
+    ap.add_argument("--ss-steps", type=int, default=4096,
+                    help="steps of the 4096^2 raster run by the hybrid (multiple of 128)")
     ap.add_argument("--tune-cache", default=None,
                     help="JSON cache of the batch autotuner (default: tune every run)")
     ap.add_argument("--side", type=int, default=N_SIDE,

@@ -1,0 +1,253 @@
+# SPDX-License-Identifier: 0BSD
+"""Training and in-loop use of the learned super-stepper.
+
+* ``make_dataset``: seeded process-map trajectories (grid side, laser power,
+  speed, spot radius, raster angle and hatch drawn per trajectory) advanced
+  by the batched FP64 solver; every 16 steps the network inputs of the field
+  and the field's change over the next 16 steps are kept (bf16 features,
+  fp32 targets, on the device).
+* ``train``: AdamW on 256 x 256 patches (batch 32), most centred near the
+  laser, through the tcgen05 training step of liblpbf_b200.
+* ``evaluate``: error of the network against the FP64 solver on held-out
+  trajectories, in kelvin, beside the error of predicting no change.
+* ``run_hybrid``: advance a field by super-steps of the network; every
+  ``judge_every`` super-steps the FP64 solver re-advances the laser window
+  (with a halo) from the block's start, and where the network's field there
+  differs by more than ``tol_K`` or its melt-pool area (T > T_melt) by more
+  than ``area_tol``, the window is rolled back to the FP64 result.
+
+CLI: ``python -m hedgehog_lpbf_b200.superstep train --out FILE`` trains and
+stores the weights (npz) with the training record.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import time
+
+import numpy as np
+import torch
+
+from . import params as P
+from . import plan as PL
+from . import process_map as PM
+from .batch import Batch, batch_opts
+from .solver import Solver
+from .surrogate import (DT_SCALE, STEPS, Net, apply, features, flatten, init_params, target,
+                        unflatten)
+
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "superstepper.npz")
+
+
+class Dataset:
+    """Per snapshot pair: inputs x4 (bf16 [side, side, 4]), target (fp32
+    [side, side]) and the laser's grid position at the pair's middle step."""
+
+    def __init__(self, x4, tgt, centre, meta):
+        self.x4, self.tgt, self.centre, self.meta = x4, tgt, centre, meta
+
+    def __len__(self):
+        return self.x4.shape[0]
+
+
+def make_dataset(n_traj: int, n_steps: int, side: int = 1024, first_index: int = 0,
+                 device="cuda:0") -> Dataset:
+    n_pairs = n_steps // STEPS
+    n_steps = n_pairs * STEPS
+    scs = PM.process_map(n_traj, n_steps, first_index=first_index, side=side)
+    dev = torch.device(device)
+    b = Batch(scs, n_steps, opts=batch_opts(depth=2, rows=(24, 48, 48, 96)), device=dev,
+              rings=False)
+    N = n_traj * n_pairs
+    x4 = torch.empty((N, side, side, 4), dtype=torch.bfloat16, device=dev)
+    tgt = torch.empty((N, side, side), dtype=torch.float32, device=dev)
+    centre = np.zeros((N, 2), dtype=np.int64)
+    T0 = [torch.empty((side, side), dtype=torch.float64, device=dev) for _ in range(n_traj)]
+    for q in range(n_pairs):
+        s0 = q * STEPS
+        for i, sc in enumerate(scs):
+            j = i * n_pairs + q
+            features(b.field(i), sc.k, sc.plan[s0:s0 + STEPS], out=x4[j])
+            T0[i].copy_(b.field(i))
+            mid = sc.plan[s0 + STEPS // 2]
+            centre[j] = (int(round(mid["y_l"] / sc.k.dy)), int(round(mid["x_l"] / sc.k.dx)))
+        b.run(s0, STEPS)
+        for i in range(n_traj):
+            target(T0[i], b.field(i), out=tgt[i * n_pairs + q])
+    torch.cuda.synchronize(dev)
+    b.close()
+    meta = {"trajectories": n_traj, "steps": n_steps, "side": side, "first_index": first_index,
+            "pairs": N}
+    return Dataset(x4, tgt, centre, meta)
+
+
+def sample(ds: Dataset, rng: np.random.Generator, batch: int, patch: int, near: float = 0.8):
+    side = ds.x4.shape[1]
+    idx = rng.integers(0, len(ds), size=batch)
+    xs, ts = [], []
+    for j in idx:
+        if rng.random() < near:
+            cy, cx = ds.centre[j] + rng.integers(-patch // 4, patch // 4 + 1, size=2)
+            y0, x0 = cy - patch // 2, cx - patch // 2
+        else:
+            y0, x0 = rng.integers(0, side - patch + 1, size=2)
+        y0 = int(np.clip(y0, 0, side - patch))
+        x0 = int(np.clip(x0, 0, side - patch))
+        xs.append(ds.x4[j, y0:y0 + patch, x0:x0 + patch])
+        ts.append(ds.tgt[j, y0:y0 + patch, x0:x0 + patch])
+    return torch.stack(xs).contiguous(), torch.stack(ts).contiguous()
+
+
+def train(net: Net, ds: Dataset, iters: int, batch: int = 32, patch: int = 256,
+          lr: float = 1e-3, weight_decay: float = 0.01, seed: int = 0, log_every: int = 200):
+    """AdamW with cosine decay from lr to lr/100; returns the loss record."""
+    rng = np.random.default_rng(seed)
+    hist = []
+    t0 = time.time()
+    for it in range(iters):
+        x, t = sample(ds, rng, batch, patch)
+        cur = lr * (0.01 + 0.99 * 0.5 * (1.0 + math.cos(math.pi * it / max(1, iters))))
+        loss = net.train_step(x, t, lr=cur, weight_decay=weight_decay)
+        if (it + 1) % log_every == 0 or it == iters - 1:
+            hist.append({"iter": it + 1, "loss": float(loss.item()), "lr": cur,
+                         "seconds": time.time() - t0})
+    torch.cuda.synchronize(net.device)
+    if net.error_word() != 0:
+        raise RuntimeError("tensor-core wait timed out during training")
+    return hist
+
+
+def evaluate(net: Net, ds: Dataset, patch: int = 256, n: int = 64, seed: int = 1):
+    """Errors (K) of the network's 16-step change on laser-centred patches,
+    beside those of predicting no change."""
+    rng = np.random.default_rng(seed)
+    err, base, sq, sqb, cnt = 0.0, 0.0, 0.0, 0.0, 0
+    for _ in range(max(1, n // 16)):
+        x, t = sample(ds, rng, 16, patch, near=1.0)
+        y = net.forward(x)
+        d = (y - t) * DT_SCALE
+        err = max(err, float(d.abs().max().item()))
+        base = max(base, float((t * DT_SCALE).abs().max().item()))
+        sq += float((d.double() ** 2).sum().item())
+        sqb += float(((t * DT_SCALE).double() ** 2).sum().item())
+        cnt += t.numel()
+    return {"max_abs_K": err, "rms_K": math.sqrt(sq / cnt),
+            "no_change_max_abs_K": base, "no_change_rms_K": math.sqrt(sqb / cnt)}
+
+
+def save(net: Net, path: str, record: dict) -> None:
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    np.savez(path, params=net.params_vector(), record=json.dumps(record))
+
+
+def load(path: str = WEIGHTS, device="cuda:0") -> tuple[Net, dict]:
+    z = np.load(path, allow_pickle=False)
+    net = Net(z["params"], device=device)
+    return net, json.loads(str(z["record"]))
+
+
+# ---- in-loop use -----------------------------------------------------------------
+
+def _window(plan, s0, s1, k, margin, nx, ny):
+    xs, ys = plan["x_l"][s0:s1], plan["y_l"][s0:s1]
+    x0 = int(math.floor(xs.min() / k.dx)) - margin
+    x1 = int(math.ceil(xs.max() / k.dx)) + margin
+    y0 = int(math.floor(ys.min() / k.dy)) - margin
+    y1 = int(math.ceil(ys.max() / k.dy)) + margin
+    return max(0, y0), min(ny, y1 + 1), max(0, x0), min(nx, x1 + 1)
+
+
+def run_hybrid(net: Net, k, plan, T0, n_steps: int, judge_every: int = 8, tol_K: float = 5.0,
+               area_tol: float = 0.02, Tm: float = 1700.0, margin: int | None = None,
+               halo: int = 32, device="cuda:0"):
+    """Super-steps of the network with the FP64 judge and rollback.  Returns
+    (field, record)."""
+    dev = torch.device(device)
+    T = torch.as_tensor(np.asarray(T0, dtype=np.float64)).to(dev).reshape(k.ny, k.nx).clone()
+    if margin is None:
+        margin = int(math.ceil(6.0 / math.sqrt(k.inv_r0_sq) / k.dx)) + 8
+    blocks = n_steps // (STEPS * judge_every)
+    rec = {"super_steps": 0, "judged": 0, "rolled_back": 0, "worst_K": 0.0,
+           "worst_area": 0.0, "fp64_window_cells": 0}
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    x4 = torch.empty((k.ny, k.nx, 4), dtype=torch.bfloat16, device=dev)
+    for blk in range(blocks):
+        s_blk = blk * STEPS * judge_every
+        wy0, wy1, wx0, wx1 = _window(plan, s_blk, s_blk + STEPS * judge_every, k, margin,
+                                     k.nx, k.ny)
+        hy0, hy1 = max(0, wy0 - halo), min(k.ny, wy1 + halo)
+        hx0, hx1 = max(0, wx0 - halo), min(k.nx, wx1 + halo)
+        Tw0 = T[hy0:hy1, hx0:hx1].clone()
+        for j in range(judge_every):
+            s = s_blk + j * STEPS
+            features(T, k, plan[s:s + STEPS], out=x4)
+            y = net.forward(x4[None])
+            apply(T, y[0])
+            rec["super_steps"] += 1
+        # FP64 judge on the window (halo cells give it the surroundings)
+        ks = P.StepConst.from_buffer_copy(bytes(k))
+        ks.nx, ks.ny = hx1 - hx0, hy1 - hy0
+        sub_plan = plan[s_blk:s_blk + STEPS * judge_every].copy()
+        sub_plan["x_l"] -= hx0 * k.dx
+        sub_plan["y_l"] -= hy0 * k.dy
+        judge = Solver(ks, Tm=Tm, device=dev, T0=Tw0.cpu().numpy())
+        judge.advance(sub_plan)
+        iy0, iy1, ix0, ix1 = wy0 - hy0, wy1 - hy0, wx0 - hx0, wx1 - hx0
+        ref = judge.field[iy0:iy1, ix0:ix1]
+        got = T[wy0:wy1, wx0:wx1]
+        diff = float((got - ref).abs().max().item())
+        a_ref = int((ref > Tm).sum().item())
+        a_got = int((got > Tm).sum().item())
+        area = abs(a_got - a_ref) / max(a_ref, 1) if (a_ref or a_got) else 0.0
+        rec["judged"] += 1
+        rec["fp64_window_cells"] += (hy1 - hy0) * (hx1 - hx0)
+        rec["worst_K"] = max(rec["worst_K"], diff)
+        rec["worst_area"] = max(rec["worst_area"], area)
+        if diff > tol_K or area > area_tol:
+            T[wy0:wy1, wx0:wx1] = ref
+            rec["rolled_back"] += 1
+    e1.record()
+    torch.cuda.synchronize(dev)
+    rec["gpu_ms"] = e0.elapsed_time(e1)
+    rec["steps"] = blocks * STEPS * judge_every
+    return T, rec
+
+
+def _cli():
+    ap = argparse.ArgumentParser(prog="python -m hedgehog_lpbf_b200.superstep")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--out", default=WEIGHTS)
+    t.add_argument("--trajectories", type=int, default=64)
+    t.add_argument("--steps", type=int, default=512)
+    t.add_argument("--side", type=int, default=1024)
+    t.add_argument("--iters", type=int, default=20000)
+    t.add_argument("--batch", type=int, default=32)
+    t.add_argument("--patch", type=int, default=256)
+    t.add_argument("--lr", type=float, default=1e-3)
+    t.add_argument("--heldout", type=int, default=8)
+    t.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args()
+    t0 = time.time()
+    ds = make_dataset(a.trajectories, a.steps, side=a.side, first_index=0)
+    held = make_dataset(a.heldout, a.steps, side=a.side, first_index=100000)
+    t_data = time.time() - t0
+    net = Net(init_params(a.seed))
+    before = evaluate(net, held, patch=a.patch)
+    hist = train(net, ds, a.iters, batch=a.batch, patch=a.patch, lr=a.lr, seed=a.seed)
+    after = evaluate(net, held, patch=a.patch)
+    rec = {"dataset": ds.meta, "heldout": held.meta, "iters": a.iters, "batch": a.batch,
+           "patch": a.patch, "lr": a.lr, "optimizer": "AdamW, cosine decay to lr/100, wd 0.01",
+           "data_seconds": t_data, "train_seconds": hist[-1]["seconds"],
+           "loss": hist, "heldout_untrained": before, "heldout_trained": after}
+    save(net, a.out, rec)
+    print(json.dumps({k: v for k, v in rec.items() if k != "loss"} |
+                     {"final_loss": hist[-1]["loss"]}))
+
+
+if __name__ == "__main__":
+    _cli()
