@@ -93,6 +93,7 @@ SIGNATURES = {
                                               ctypes.c_size_t, _vp, ctypes.POINTER(_vp)]),
     "lpbf_b200_batch_run": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
     "lpbf_b200_batch_capture": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "lpbf_b200_batch_run_wsub": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "lpbf_b200_batch_result_in_b": (ctypes.c_int, [_vp]),
     "lpbf_b200_batch_launches": (ctypes.c_int, [_vp, ctypes.c_int]),
     "lpbf_b200_batch_tasks": (ctypes.c_int, [_vp]),

@@ -373,6 +373,59 @@ bool batch_layout(const lpbf_b200_scenario* sc, int n, int n_steps,
 
 }  // namespace lpbf_b200
 
+namespace lpbf_b200 {
+
+// ---- sub-grid melt width on the hot column ------------------------------------
+
+// Per scenario (one CTA each), after plan step `step` wrote its Partial and
+// the field now sits in buf[par]: the melt width through the column of the
+// step's hottest cell, interpolating the two T = Tm crossings linearly (the
+// rule of the reference's MetricsTask, include/gpu_step_task.hpp:380-395),
+// where cruise[step][user] is set and the peak exceeds Tm; 0 elsewhere.
+__global__ void wsub_kernel(const BatchScen* scen, int step, int n_steps, int par,
+                            const unsigned char* cruise, double* w_sub, int nscen) {
+    __shared__ int s_a, s_b;
+    const BatchScen& sc = scen[blockIdx.x];
+    const int user = sc.user;
+    const int nx = sc.par.c.nx, ny = sc.par.c.ny;
+    const double Tm = sc.par.c.Tm, dy = sc.par.c.dy;
+    const bool has = sc.ring != nullptr && cruise[(size_t)step * nscen + user] != 0;
+    const Partial r = has ? sc.ring[step] : Partial{-1.0, 0, 0, -1};
+    if (!(has && r.tmax > Tm)) {
+        if (threadIdx.x == 0) w_sub[(size_t)step * nscen + user] = 0.0;
+        return;
+    }
+    const int x = (int)(r.arg % nx);
+    const double* col = sc.buf[par] + x;
+    if (threadIdx.x == 0) { s_a = ny; s_b = -1; }
+    __syncthreads();
+    int a = ny, b = -1;
+    for (int y = threadIdx.x; y < ny; y += blockDim.x)
+        if (col[(size_t)y * nx] > Tm) { a = min(a, y); b = max(b, y); }
+    atomicMin(&s_a, a);
+    atomicMax(&s_b, b);
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    a = s_a;
+    b = s_b;
+    double w = 0.0;
+    if (b >= 0) {
+        double lo = __dmul_rn((double)a, dy), hi = __dmul_rn((double)b, dy);
+        if (a > 0) {
+            const double c0 = col[(size_t)(a - 1) * nx], c1 = col[(size_t)a * nx];
+            lo = __dmul_rn(__dadd_rn((double)(a - 1), __ddiv_rn(__dsub_rn(Tm, c0), __dsub_rn(c1, c0))), dy);
+        }
+        if (b < ny - 1) {
+            const double c0 = col[(size_t)b * nx], c1 = col[(size_t)(b + 1) * nx];
+            hi = __dmul_rn(__dadd_rn((double)b, __ddiv_rn(__dsub_rn(Tm, c0), __dsub_rn(c1, c0))), dy);
+        }
+        w = __dmul_rn(__dsub_rn(hi, lo), 1e6);
+    }
+    w_sub[(size_t)step * nscen + user] = w;
+}
+
+}  // namespace lpbf_b200
+
 // ===========================================================================
 // C-ABI
 // ===========================================================================
@@ -384,6 +437,7 @@ struct lpbf_b200_batch {
     BatchLayout lay;
     unsigned char* work = nullptr;
     int cur = 0;                   // buffer holding the current fields (0: T_a, 1: T_b)
+    bool all_rings = false;        // every scenario has a ring
     int device = 0;
     // cached graphs, keyed by (first_step, n_steps, starting parity)
     struct Graph { cudaGraphExec_t exec = nullptr; int first = -1, n = -1, par = -1; };
@@ -524,6 +578,7 @@ int lpbf_b200_batch_create(const lpbf_b200_scenario* sc, int n_scen, int n_steps
         b.buf[0] = s.T_a;
         b.buf[1] = s.T_b;
         b.ring = s.ring;
+        b.user = lay.order[i];
         if (stage == BATCH_STAGE_TMAP &&
             (!tensor_map_f64(s.T_a, k.nx, k.ny, ADV_COLS, ADV_R, &b.map[0]) ||
              !tensor_map_f64(s.T_b, k.nx, k.ny, ADV_COLS, ADV_R, &b.map[1])))
@@ -556,6 +611,8 @@ int lpbf_b200_batch_create(const lpbf_b200_scenario* sc, int n_scen, int n_steps
     b->K = lay.K;
     b->ctas_per_sm = o.ctas_per_sm;
     b->stage = stage;
+    b->all_rings = true;
+    for (int i = 0; i < n_scen; ++i) b->all_rings = b->all_rings && sc[i].ring != nullptr;
     b->lay = std::move(lay);
     b->work = w;
     b->device = dev;
@@ -627,6 +684,22 @@ int lpbf_b200_batch_run(lpbf_b200_batch* b, int first_step, int n_steps, int use
     if (!g) return LPBF_ERR_CUDA;
     if (cudaGraphLaunch(g->exec, stream) != cudaSuccess) return LPBF_ERR_CUDA;
     b->cur = par ^ (((n_steps + b->K - 1) / b->K) & 1);
+    return LPBF_OK;
+}
+
+int lpbf_b200_batch_run_wsub(lpbf_b200_batch* b, int first_step, int n_steps,
+                             const unsigned char* cruise, double* w_sub, cudaStream_t stream) {
+    if (!valid_range(b, first_step, n_steps) || !cruise || !w_sub || !b->all_rings)
+        return LPBF_ERR_ARG;
+    const BatchScen* scen = reinterpret_cast<const BatchScen*>(b->work + b->lay.off_scen);
+    for (int s = first_step; s < first_step + n_steps; ++s) {
+        int par = b->cur;
+        if (b->issue(s, 1, par, stream, &par) != cudaSuccess) return LPBF_ERR_CUDA;
+        b->cur = par;
+        wsub_kernel<<<b->nscen, 128, 0, stream>>>(scen, s, b->n_steps, par, cruise, w_sub,
+                                                  b->nscen);
+        if (cudaGetLastError() != cudaSuccess) return LPBF_ERR_CUDA;
+    }
     return LPBF_OK;
 }
 

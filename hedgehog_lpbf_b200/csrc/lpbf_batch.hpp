@@ -48,6 +48,7 @@ struct alignas(128) BatchScen {
     AdvParams par;                 // static launch parameters (laser, band, buffers patched per task)
     double* buf[2];                // the ping-pong pair
     Partial* ring;                 // one Partial per plan step, or null
+    int user;                      // the caller's index of this scenario
 };
 static_assert(offsetof(BatchScen, par) % 8 == 0 && sizeof(AdvParams) % 8 == 0, "8-byte words");
 

@@ -192,6 +192,15 @@ int lpbf_b200_batch_run(lpbf_b200_batch* b, int first_step, int n_steps, int use
  * use_graph != 0 would replay for these steps from the current buffers, so
  * that the first such run pays no capture.  Not itself capturable. */
 int lpbf_b200_batch_capture(lpbf_b200_batch* b, int first_step, int n_steps);
+/* Advance steps [first_step, first_step + n_steps) one step per launch and,
+ * after each step s, write w_sub[s * n_scen + i] (device f64, caller order):
+ * scenario i's sub-grid melt width [um] through the column of that step's
+ * hottest cell, from the two linearly interpolated T = Tm crossings (the
+ * reference MetricsTask rule, include/gpu_step_task.hpp:380-395), where
+ * cruise[s * n_scen + i] (device bytes) is non-zero and the step's peak
+ * exceeds Tm, else 0.  Every scenario needs a ring. */
+int lpbf_b200_batch_run_wsub(lpbf_b200_batch* b, int first_step, int n_steps,
+                             const unsigned char* cruise, double* w_sub, cudaStream_t stream);
 /* 1 when the current fields are in the T_b buffers, 0 for T_a. */
 int lpbf_b200_batch_result_in_b(const lpbf_b200_batch* b);
 /* Launches that a run of n_steps issues; queue items per launch; rows per

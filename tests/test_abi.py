@@ -79,3 +79,20 @@ def test_gpu_step_task_header_builds_against_library():
     if os.path.isdir(os.path.join(ref, "src", "gpu")):
         subprocess.run(["make", "-s", "-C", d, "ref", f"REF={ref}"], check=True)
         assert os.path.exists(os.path.join(ROOT, "tests", "_build", "ref_hhcuda_on_b200"))
+
+
+def test_manifest_driver_rejects_unusable_manifests(tmp_path):
+    """Exit status 4 before any CUDA call, as the reference's manifest mode."""
+    d = os.path.join(ROOT, "tests", "dropin")
+    subprocess.run(["make", "-s", "-C", d, "demo"], check=True)
+    exe = os.path.join(ROOT, "tests", "_build", "manifest_batched")
+    r = subprocess.run([exe, f"--manifest={tmp_path / 'nope.csv'}"], capture_output=True, text=True)
+    assert r.returncode == 4 and "cannot open manifest" in r.stderr
+    bad = tmp_path / "bad.csv"
+    bad.write_text("run_id,cond_id,draw_id,config,P_W,V_mps,r0_m,eta,dsub_m,physics\nr,c,d,b,200,1,5e-5,0.4,3e-5,base\n")
+    r = subprocess.run([exe, f"--manifest={bad}"], capture_output=True, text=True)
+    assert r.returncode == 4 and "missing column 'kmult'" in r.stderr
+    empty = tmp_path / "empty.csv"
+    empty.write_text("")
+    r = subprocess.run([exe, f"--manifest={empty}"], capture_output=True, text=True)
+    assert r.returncode == 4

@@ -118,3 +118,63 @@ def test_reference_driver_on_this_library(gpu, tmp_path):
         meta = json.load(open(out / "meta.json"))
         assert _fmt(meta["peak_T_K"]) == _fmt(g["meta"]["peak_T_K"])
         assert _fmt(meta["peak_W_um"]) == _fmt(g["meta"]["peak_W_um"])
+
+
+# ---- manifest ensembles on the batched kernel --------------------------------
+
+_MCOLS = ["physics", "run_id", "P_W", "V_mps", "r0_m", "cond_id", "draw_id", "config", "eta",
+          "dsub_m", "kmult"]          # shuffled: columns are matched by name
+
+
+def _write_manifest(path, rows):
+    with open(path, "w") as f:
+        f.write(",".join(_MCOLS) + "\n")
+        for r in rows:
+            f.write(",".join(str(r[c]) for c in _MCOLS) + "\n")
+
+
+def _manifest_rows():
+    rng = np.random.default_rng(5)
+    rows = []
+    for i in range(10):
+        rows.append({"run_id": f"r{i}", "cond_id": f"c{i % 3}", "draw_id": f"d{i}",
+                     "config": "base", "P_W": round(150 + 200 * rng.random(), 3),
+                     "V_mps": round(0.6 + 0.8 * rng.random(), 3),
+                     "r0_m": f"{25e-6 + 25e-6 * rng.random():.4e}",
+                     "eta": round(0.3 + 0.15 * rng.random(), 3),
+                     "dsub_m": f"{20e-6 + 20e-6 * rng.random():.4e}", "kmult": 1,
+                     "physics": "base"})
+    rows.append(dict(rows[0], run_id="x0", physics="ext", config="ext", kmult=1))
+    rows.append(dict(rows[1], run_id="x1", physics="ext", config="ext", kmult=2.5))
+    return rows
+
+
+def _results(text):
+    return {ln.split(",")[1]: ln.strip().split(",") for ln in text.splitlines()
+            if ln.startswith("RESULT,")}
+
+
+def test_manifest_batched_matches_reference_manifest(gpu, tmp_path):
+    """The reference's --manifest loop (its own hh_gpu_main.cpp on this
+    library, one graph per row) and include/manifest.hpp (baseline rows in one
+    batch, melt widths on the device) print the same RESULT fields: constants,
+    steady sub-grid melt width, peak T and step count (wall time aside)."""
+    ref = os.path.join(BUILD, "ref_hhcuda_on_b200")
+    if not os.path.exists(ref):
+        pytest.skip("reference driver not built (needs the reference tree at build time)")
+    _demo()
+    ours = os.path.join(BUILD, "manifest_batched")
+    man = tmp_path / "runs.csv"
+    rows = _manifest_rows()
+    _write_manifest(man, rows)
+    r_ref = subprocess.run([ref, f"--manifest={man}"], check=True, timeout=600,
+                           capture_output=True, text=True).stdout
+    r_our = subprocess.run([ours, f"--manifest={man}"], check=True, timeout=600,
+                           capture_output=True, text=True).stdout
+    a, b = _results(r_ref), _results(r_our)
+    assert sorted(a) == sorted(b) == sorted(r["run_id"] for r in rows)
+    for rid in a:
+        assert a[rid][:14] == b[rid][:14], (rid, a[rid], b[rid])      # all but wall_ms
+        assert a[rid][15] == b[rid][15]                                # n_steps
+        assert float(b[rid][13]) > 1000.0                              # the beam heated it
+    assert any(float(b[r][12]) > 0.0 for r in b)                       # some melt widths
