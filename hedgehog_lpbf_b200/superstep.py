@@ -231,7 +231,31 @@ def _cli():
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--heldout", type=int, default=8)
     t.add_argument("--seed", type=int, default=0)
+    f = sub.add_parser("forward", help="time the network's forward pass on a side x side field")
+    f.add_argument("--side", type=int, default=4096)
+    f.add_argument("--reps", type=int, default=5)
     a = ap.parse_args()
+    if a.cmd == "forward":
+        net = load()[0] if os.path.exists(WEIGHTS) else Net(init_params(0))
+        mat, pr = P.benchmark_material_process()
+        dom = P.square_domain(a.side)
+        k = P.make_const(mat, pr, dom, P.dt_fraction(mat, dom))
+        plan = PL.raster_for_steps(dom, k.dt, 64, V=1.0, hatch=100e-6, n_tracks=2)
+        T = torch.full((a.side, a.side), 300.0, dtype=torch.float64, device="cuda")
+        x4 = features(T, k, plan)[None]
+        y = net.forward(x4)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.reps):
+            net.forward(x4, y)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.reps
+        flop = 2 * 9 * (4 * 32 + 3 * 32 * 32 + 32) * a.side * a.side
+        print(json.dumps({"side": a.side, "ms": ms, "tflops": flop / (ms * 1e-3) / 1e12,
+                          "error_word": net.error_word()}))
+        return
     t0 = time.time()
     ds = make_dataset(a.trajectories, a.steps, side=a.side, first_index=0)
     held = make_dataset(a.heldout, a.steps, side=a.side, first_index=100000)
