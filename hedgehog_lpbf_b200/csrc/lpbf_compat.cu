@@ -32,25 +32,39 @@ __constant__ double c_T_PTS[9]  = {298, 473, 673, 873, 1073, 1273, 1473, 1533, 1
 __constant__ double c_K_PTS[9]  = {8.9, 12.9, 15.8, 18.7, 21.9, 25.6, 28.6, 29.3, 29.6};
 __constant__ double c_CP_PTS[9] = {435, 479, 515, 558, 580, 628, 670, 685, 720};
 constexpr double T_SOL = 1533.0, T_LIQ = 1609.0, LATENT = 210.0e3;
+constexpr double INV_MUSHY = 1.0 / (T_LIQ - T_SOL);
 
-// params.hpp:75-83: clamped piecewise-linear lookup.
-__device__ __forceinline__ double tab_interp(double T, const double* ys) {
-    if (T <= c_T_PTS[0]) return ys[0];
-    if (T >= c_T_PTS[8]) return ys[8];
+// The tables in shared memory (lanes index them divergently): temperatures,
+// k, cp, and the reciprocal segment widths.
+struct ExtTab { double t[9], k[9], cp[9], inv[8]; };
+
+// params.hpp:75-89: clamped piecewise-linear lookup.  The segment comes from
+// seven compares instead of a search loop, and the segment width's
+// reciprocal replaces the division (an ulp-level difference).
+__device__ __forceinline__ int ext_seg(const ExtTab& tb, double T) {
     int i = 1;
-    while (T > c_T_PTS[i]) ++i;
-    const double f = (T - c_T_PTS[i - 1]) / (c_T_PTS[i] - c_T_PTS[i - 1]);
+#pragma unroll
+    for (int j = 1; j < 8; ++j) i += (T > tb.t[j]) ? 1 : 0;
+    return i;
+}
+__device__ __forceinline__ double ext_interp(const ExtTab& tb, const double* ys, double T, int i) {
+    if (T <= tb.t[0]) return ys[0];
+    if (T >= tb.t[8]) return ys[8];
+    const double f = (T - tb.t[i - 1]) * tb.inv[i - 1];
     return ys[i - 1] + f * (ys[i] - ys[i - 1]);
 }
-__device__ __forceinline__ double k_eff_d(double T, double kmult) {
-    const double k = tab_interp(T, c_K_PTS);
+// k_of(T) * k_enh(T, kmult)  (params.hpp:91-105)
+__device__ __forceinline__ double ext_k(const ExtTab& tb, double T, double kmult, double* k_plain) {
+    const double k = ext_interp(tb, tb.k, T, ext_seg(tb, T));
+    if (k_plain) *k_plain = k;
     if (kmult <= 1.0) return k;
-    const double s = (T <= T_SOL) ? 0.0 : (T >= T_LIQ) ? 1.0 : (T - T_SOL) / (T_LIQ - T_SOL);
+    const double s = (T <= T_SOL) ? 0.0 : (T >= T_LIQ) ? 1.0 : (T - T_SOL) * INV_MUSHY;
     return k * (1.0 + (kmult - 1.0) * s);
 }
-__device__ __forceinline__ double cp_eff_d(double T) {
-    double c = tab_interp(T, c_CP_PTS);
-    if (T >= T_SOL && T <= T_LIQ) c += LATENT / (T_LIQ - T_SOL);
+// cp_of(T) plus the latent heat spread over the mushy range (params.hpp:106-110)
+__device__ __forceinline__ double ext_cp(const ExtTab& tb, double T) {
+    double c = ext_interp(tb, tb.cp, T, ext_seg(tb, T));
+    if (T >= T_SOL && T <= T_LIQ) c += LATENT * INV_MUSHY;
     return c;
 }
 
@@ -90,35 +104,71 @@ struct ExtParams {
     long long ref_nparts;
 };
 
-// One thread per cell, 16 x 16 blocks (the reference's layout, so the
-// reference fused-reduce array has exactly one entry per block).  The cell
-// arithmetic follows include/step_task.hpp:144-184.
+// Blocks of 16 x 16 threads over tiles of 16 x EXT_ROWS cells (each thread
+// owns EXT_ROWS / 16 cells of one column).  The block stages the tile's T
+// plus a one-cell ring (edge neighbours mirrored: the ghost is the centre)
+// and the conductivities k_eff(T) of all of them in shared memory, so each
+// cell's k_eff is evaluated once and read by its four neighbours.  The cell
+// arithmetic follows include/step_task.hpp:144-184, with the divisions by
+// dSub and by rho cp_eff(T) done as multiplications by correctly rounded
+// reciprocals (ulp-level differences).  For the reference's fused-reduce
+// layout (one Partial per 16 x 16 block) a tile writes its result into its
+// first 16 x 16 entry and the neutral element into the others.
+constexpr int EXT_ROWS = 64;
+constexpr int EXT_RPT = EXT_ROWS / 16;          // cells per thread
+
 template <bool REDUCE>
 __global__ void __launch_bounds__(256)
 ext_step_kernel(const double* __restrict__ Tin, double* __restrict__ Tout,
                 const __grid_constant__ ExtParams p) {
     const StepConst& k = p.k;
-    const int x = blockIdx.x * 16 + threadIdx.x;
-    const int y = blockIdx.y * 16 + threadIdx.y;
+    __shared__ double sT[EXT_ROWS + 2][18], sK[EXT_ROWS + 2][18];
+    __shared__ ExtTab tb;
+    const int tid = threadIdx.y * 16 + threadIdx.x;
     const int nx = k.nx, ny = k.ny;
     const long long N = (long long)nx * ny;
-    double v = -1.0;
-    bool inside = x < nx && y < ny;
-    if (inside) {
+    if (tid < 9) {
+        tb.t[tid] = c_T_PTS[tid];
+        tb.k[tid] = c_K_PTS[tid];
+        tb.cp[tid] = c_CP_PTS[tid];
+        if (tid < 8) tb.inv[tid] = 1.0 / (c_T_PTS[tid + 1] - c_T_PTS[tid]);
+    }
+    __syncthreads();
+    const int bx = blockIdx.x * 16, by = blockIdx.y * EXT_ROWS;
+    for (int e = tid; e < (EXT_ROWS + 2) * 18; e += 256) {
+        const int i = e % 18, j = e / 18;
+        const int gx = min(max(bx + i - 1, 0), nx - 1);
+        const int gy = min(max(by + j - 1, 0), ny - 1);
+        const double T = __ldg(Tin + (size_t)gy * nx + gx);
+        sT[j][i] = T;
+        sK[j][i] = ext_k(tb, T, k.kmult, nullptr);
+    }
+    __syncthreads();
+    const double r_dsub = __drcp_rn(k.dSub);
+    const double Ta4 = k.Tamb * k.Tamb * k.Tamb * k.Tamb;
+    const int tx = threadIdx.x;
+    const int x = bx + tx;
+    double tm = -1.0;
+    long long ag = N;
+    int mn = ny, mx = -1;
+#pragma unroll 1
+    for (int q = 0; q < EXT_RPT; ++q) {
+        const int ty = threadIdx.y + 16 * q;            // rows of a thread step by 16
+        const int y = by + ty;
+        if (!(x < nx && y < ny)) continue;
         const long long c = (long long)y * nx + x;
+        double v;
         if (p.bc == 1 && (x == 0 || y == 0 || x == nx - 1 || y == ny - 1)) {
             v = p.T_edge;
         } else {
-            const double T = Tin[c];
-            const double Txm = (x == 0) ? T : Tin[c - 1];
-            const double Txp = (x == nx - 1) ? T : Tin[c + 1];
-            const double Tym = (y == 0) ? T : Tin[c - nx];
-            const double Typ = (y == ny - 1) ? T : Tin[c + nx];
-            const double kC = k_eff_d(T, k.kmult);
-            const double kxm = 0.5 * (kC + k_eff_d(Txm, k.kmult));
-            const double kxp = 0.5 * (kC + k_eff_d(Txp, k.kmult));
-            const double kym = 0.5 * (kC + k_eff_d(Tym, k.kmult));
-            const double kyp = 0.5 * (kC + k_eff_d(Typ, k.kmult));
+            const double T = sT[ty + 1][tx + 1];
+            const double Txm = sT[ty + 1][tx], Txp = sT[ty + 1][tx + 2];
+            const double Tym = sT[ty][tx + 1], Typ = sT[ty + 2][tx + 1];
+            const double kC = sK[ty + 1][tx + 1];
+            const double kxm = 0.5 * (kC + sK[ty + 1][tx]);
+            const double kxp = 0.5 * (kC + sK[ty + 1][tx + 2]);
+            const double kym = 0.5 * (kC + sK[ty][tx + 1]);
+            const double kyp = 0.5 * (kC + sK[ty + 2][tx + 1]);
             const double div = (kxp * (Txp - T) - kxm * (T - Txm)) * k.inv_dx2
                              + (kyp * (Typ - T) - kym * (T - Tym)) * k.inv_dy2;
             const double xd = __dsub_rn(__dmul_rn((double)x, k.dx), k.x_l);
@@ -130,35 +180,49 @@ ext_step_kernel(const double* __restrict__ Tin, double* __restrict__ Tout,
             double q_top = k.hConv * (T - k.Tamb);
             if (k.radiation) {
                 const double T4 = T * T * T * T;
-                const double Ta4 = k.Tamb * k.Tamb * k.Tamb * k.Tamb;
                 q_top += k.eps * SIGMA_SB * (T4 - Ta4);
             }
-            const double q_bot = (tab_interp(T, c_K_PTS) / k.dSub) * (T - k.Tsub);
+            // one table segment for the substrate conductivity (no kmult) and cp
+            const int sg = ext_seg(tb, T);
+            const double k_plain = k.kmult <= 1.0 ? kC : ext_interp(tb, tb.k, T, sg);
+            double cp = ext_interp(tb, tb.cp, T, sg);
+            if (T >= T_SOL && T <= T_LIQ) cp += LATENT * INV_MUSHY;
+            const double q_bot = (k_plain * r_dsub) * (T - k.Tsub);
             const double rhs = div + (q_in - q_top - q_bot) * k.inv_h;
-            v = T + k.dt * rhs / (k.rho * cp_eff_d(T));
+            v = T + (k.dt * rhs) * __drcp_rn(k.rho * cp);
         }
         Tout[c] = v;
+        if constexpr (REDUCE) {
+            // rows of this thread come in increasing order: strict '>' keeps
+            // the first (smallest-index) maximum; NaN never wins
+            if (v > tm) { tm = v; ag = c; }
+            if (v > p.Tm) { mn = min(mn, y); mx = max(mx, y); }
+        }
     }
     if constexpr (REDUCE) {
-        double tm = inside ? v : -1.0;
-        long long ag = inside ? (long long)y * nx + x : N;
-        int mn = ny, mx = -1;
-        if (inside && v > p.Tm) { mn = y; mx = y; }
-        if (!(tm > -1.0)) { tm = -1.0; ag = N; }   // NaN and values <= -1 never win
         partial_warp_reduce(tm, ag, mn, mx);
         __shared__ Partial red[8];
         __shared__ unsigned int s_last;
-        const int tid = threadIdx.y * 16 + threadIdx.x;
         if ((tid & 31) == 0) red[tid >> 5] = Partial{tm, ag, mn, mx};
         __syncthreads();
-        const int bid = blockIdx.y * gridDim.x + blockIdx.x;
         const int nblk = gridDim.x * gridDim.y;
         if (tid == 0) {
             double a = -1.0; long long b = N; int c1 = ny, d1 = -1;
             for (int w = 0; w < 8; ++w)
                 partial_take(a, b, c1, d1, red[w].tmax, red[w].arg, red[w].ymin, red[w].ymax);
-            if (p.ref_out) p.ref_out[bid] = Partial{a, b, c1, d1};
-            else p.scratch[bid] = Partial{a, b, c1, d1};
+            if (p.ref_out) {
+                // reference layout: 16 x 16 blocks, row-major over the grid
+                const int gx16 = (nx + 15) / 16, gy16 = (ny + 15) / 16;
+                const Partial neutral{-1.0, N, ny, -1};
+                for (int q = 0; q < EXT_RPT; ++q) {
+                    const int yb = blockIdx.y * EXT_RPT + q;
+                    if (yb >= gy16) break;
+                    const long long idx = (long long)yb * gx16 + blockIdx.x;
+                    if (idx < p.ref_nparts) p.ref_out[idx] = q == 0 ? Partial{a, b, c1, d1} : neutral;
+                }
+            } else {
+                p.scratch[blockIdx.y * gridDim.x + blockIdx.x] = Partial{a, b, c1, d1};
+            }
         }
         if (p.ref_out) return;
         __threadfence();
@@ -169,9 +233,9 @@ ext_step_kernel(const double* __restrict__ Tin, double* __restrict__ Tout,
         __threadfence();
         double a = -1.0; long long b = N; int c1 = ny, d1 = -1;
         for (int i = tid; i < nblk; i += 256) {
-            const Partial* q = &p.scratch[i];
-            partial_take(a, b, c1, d1, __ldcg(&q->tmax), __ldcg(&q->arg), __ldcg(&q->ymin),
-                         __ldcg(&q->ymax));
+            const Partial* qq = &p.scratch[i];
+            partial_take(a, b, c1, d1, __ldcg(&qq->tmax), __ldcg(&qq->arg), __ldcg(&qq->ymin),
+                         __ldcg(&qq->ymax));
         }
         partial_warp_reduce(a, b, c1, d1);
         __syncthreads();
@@ -194,7 +258,7 @@ cudaError_t launch_ext_step(const double* Tin, double* Tout, const StepConst& k,
     p.k = k; p.bc = bc; p.T_edge = T_edge; p.Tm = Tm;
     p.ring = ring; p.ref_out = ref_out; p.ref_nparts = ref_nparts;
     const dim3 blk(16, 16);
-    const dim3 grd((k.nx + 15) / 16, (k.ny + 15) / 16);
+    const dim3 grd((k.nx + 15) / 16, (k.ny + EXT_ROWS - 1) / EXT_ROWS);
     const bool reduce = ring || ref_out;
     if (reduce && !ref_out) {
         if (!ws) return cudaErrorInvalidValue;
