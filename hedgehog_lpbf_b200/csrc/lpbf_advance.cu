@@ -100,6 +100,24 @@ bool tensor_map_f32(const void* base, int nx, int ny, int box_cols, int box_rows
                       32, out);
 }
 
+// NHWC bf16 activations (C channels per pixel) as a 4D tensor (c, x, y, b):
+// boxes of {C, box_px, 1, 1} with the 64-byte swizzle that the tensor core's
+// K-major SW64 operand layout expects; out-of-range pixels read as zero.
+bool tensor_map_act_bf16(const void* base, int C, int W, int H, int B, int box_px,
+                         CUtensorMap* out) {
+    EncodeFn fn = encode_fn();
+    if (!fn || C * 2 > 64 || (C * 2) % 16 != 0) return false;
+    cuuint64_t gdim[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+    cuuint64_t gstride[3] = {(cuuint64_t)C * 2, (cuuint64_t)C * 2 * W, (cuuint64_t)C * 2 * W * H};
+    cuuint32_t box[4] = {(cuuint32_t)C, (cuuint32_t)box_px, 1, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    std::memset(out, 0, sizeof(*out));
+    return fn(out, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), gdim, gstride,
+              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+}
+
 // ---- launch of one temporally blocked step ---------------------------------
 namespace {
 

@@ -39,6 +39,8 @@ bool tensor_map_f64(const void* base, int nx, int ny, int box_cols, int box_rows
                     CUtensorMap* out);
 bool tensor_map_f32(const void* base, int nx, int ny, int box_cols, int box_rows,
                     CUtensorMap* out);
+bool tensor_map_act_bf16(const void* base, int C, int W, int H, int B, int box_px,
+                         CUtensorMap* out);
 
 // Rows whose source term can be non-zero in any of the K substeps (a
 // superset: the kernel decides exactly, this only routes rows to the general

@@ -17,6 +17,9 @@
 // ---------------------------------------------------------------------------
 #include <cstring>
 
+#include <algorithm>
+
+#include "lpbf_host.hpp"
 #include "lpbf_surrogate.cuh"
 #include "lpbf_b200.h"
 
@@ -63,6 +66,25 @@ __device__ __forceinline__ void fill_a(bf16* sA, const ConvArgs& a, int b, int y
                 v = __ldg(reinterpret_cast<const uint4*>(
                     X + ((size_t(b) * a.H + yy) * a.W + xx) * 32 + c * 8));
             *reinterpret_cast<uint4*>(T::a_at(sA, m, tap * 32 + c * 8)) = v;
+        }
+    } else if constexpr (CIN == 4) {
+        // K = 64: k = tap * 4 + ci; a 16-byte unit j holds taps 2j and 2j + 1
+        // (one 8-byte pixel load each); units past tap 8 are zero
+        const uint2* X = static_cast<const uint2*>(a.x);
+        for (int u = tid; u < 128 * 8; u += blockDim.x) {
+            const int m = u >> 3, j = u & 7;
+            uint2 h[2] = {make_uint2(0u, 0u), make_uint2(0u, 0u)};
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int tap = 2 * j + q;
+                if (tap < 9) {
+                    const int yy = y + tap / 3 - 1, xx = x0 + m + tap % 3 - 1;
+                    if (yy >= 0 && yy < a.H && xx >= 0 && xx < a.W)
+                        h[q] = __ldg(X + (size_t(b) * a.H + yy) * a.W + xx);
+                }
+            }
+            *reinterpret_cast<uint4*>(T::a_at(sA, m, j * 8)) =
+                make_uint4(h[0].x, h[0].y, h[1].x, h[1].y);
         }
     } else {
         // K = 64: k = tap * CIN + ci for k < 9 * CIN, zero beyond; unit = 8 k
@@ -234,6 +256,179 @@ __global__ void __launch_bounds__(128) gemm_bt_kernel(const bf16* A, const bf16*
     if (warp == 0) tmem_free(tmem, T::TMEM_COLS);
 }
 
+// ---- 32-channel layers: TMA-fed, warp-specialized, persistent --------------
+//
+// One CTA per SM walks the tiles (128 pixels of one row) of the layer.  Warp 0
+// (one thread) loads each tile's nine tap tiles with TMA from a 4D tensor map
+// over the NHWC activations: box {32 channels, 128 pixels}, 64-byte swizzle,
+// i.e. exactly the tensor core's K-major SW64 operand layout; pixels off the
+// image read as zero (the padding).  Warp 1 issues the 18 MMAs of a tile
+// into one of two TMEM accumulators and commits to the stage's "empty" and
+// the accumulator's "full" barriers.  Warps 2-5 read their 32 accumulator
+// lanes and run the epilogue, then release the accumulator.  Two shared
+// memory stages and two accumulators overlap loads, MMAs and epilogues.
+// Every wait is bounded; a timeout sets the error word and ends the CTA.
+constexpr int CT_STAGES = 2;
+constexpr int CT_TAP_ELEMS = 128 * 32;
+constexpr int CT_STAGE_BYTES = 9 * CT_TAP_ELEMS * 2;
+constexpr int CT_THREADS = 192;
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1,
+                                            int c2, int c3, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        :: "r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2),
+           "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+
+template <int N>
+constexpr size_t ct_smem_bytes() {
+    return 1024 + size_t(CT_STAGES) * CT_STAGE_BYTES + size_t(N) * 288 * 2;
+}
+
+template <int N, int EPI>
+__global__ void __launch_bounds__(CT_THREADS, 1)
+conv_tma_kernel(const __grid_constant__ CUtensorMap xmap, const ConvArgs a, int ntiles,
+                int xtiles) {
+    using T = TileMma<N, 288, 32>;
+    constexpr int ACC_COLS = T::TMEM_COLS;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ uint64_t full[CT_STAGES], empty[CT_STAGES], tfull[2], tempty[2];
+    __shared__ uint32_t tslot;
+    uint8_t* base = align1024(smem_raw);
+    bf16* sA = reinterpret_cast<bf16*>(base);
+    bf16* sB = reinterpret_cast<bf16*>(base + size_t(CT_STAGES) * CT_STAGE_BYTES);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (warp == 1) tmem_alloc(&tslot, 2 * ACC_COLS);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < CT_STAGES; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
+        for (int i = 0; i < 2; ++i) { mbar_init(&tfull[i], 1); mbar_init(&tempty[i], 4); }
+        fence_mbar_init();
+    }
+    fill_b<N, 288, T>(sB, a.w);
+    fence_smem_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tslot;
+    bool ok = true;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            for (int i = 0, t = blockIdx.x; t < ntiles; ++i, t += gridDim.x) {
+                const int s = i % CT_STAGES;
+                const uint32_t ph = (i / CT_STAGES) & 1;
+                if (!mbar_wait_bounded(&empty[s], ph ^ 1)) { ok = false; break; }
+                const int xt = t % xtiles, row = t / xtiles;
+                const int y = row % a.H, b = row / a.H, x0 = xt * 128;
+                mbar_expect_tx(&full[s], CT_STAGE_BYTES);
+                bf16* st = sA + size_t(s) * 9 * CT_TAP_ELEMS;
+#pragma unroll 1
+                for (int tap = 0; tap < 9; ++tap)
+                    tma_load_4d(st + tap * CT_TAP_ELEMS, &xmap, 0, x0 + tap % 3 - 1,
+                                y + tap / 3 - 1, b, &full[s]);
+            }
+        }
+    } else if (warp == 1) {
+        for (int i = 0, t = blockIdx.x; t < ntiles; ++i, t += gridDim.x) {
+            const int s = i % CT_STAGES;
+            const uint32_t ph = (i / CT_STAGES) & 1;
+            const int acc = i & 1;
+            const uint32_t aph = (i >> 1) & 1;
+            bool w = mbar_wait_bounded(&tempty[acc], aph ^ 1);
+            w = w && mbar_wait_bounded(&full[s], ph);
+            if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
+            tc_fence_after();
+            T::issue(sA + size_t(s) * 9 * CT_TAP_ELEMS, sB, tmem + acc * ACC_COLS, &empty[s]);
+            cutlass::arch::umma_arrive(&tfull[acc]);
+        }
+    } else {
+        const int q = warp & 3;                      // TMEM lane quarter of this warp
+        for (int i = 0, t = blockIdx.x; t < ntiles; ++i, t += gridDim.x) {
+            const int acc = i & 1;
+            const uint32_t aph = (i >> 1) & 1;
+            if (!__all_sync(0xffffffffu, mbar_wait_bounded(&tfull[acc], aph))) { ok = false; break; }
+            tc_fence_after();
+            float v[32];
+            const uint32_t addr = tmem + acc * ACC_COLS + (uint32_t(q * 32) << 16);
+            if constexpr (N == 32) tmem_ld32(addr, v);
+            else tmem_ld16(addr, v);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[acc]);
+            const int xt = t % xtiles, row = t / xtiles;
+            const int y = row % a.H, b = row / a.H;
+            const int x = xt * 128 + q * 32 + lane;
+            if (x >= a.W) continue;
+            const size_t p = (size_t(b) * a.H + y) * a.W + x;
+            if constexpr (EPI == EPI_LINEAR) {
+                static_cast<float*>(a.out)[p] = v[0] + (a.bias ? a.bias[0] : 0.0f);
+            } else {
+                uint32_t o[N / 2], pr[N / 2];
+#pragma unroll
+                for (int c = 0; c < N; c += 2) {
+                    float v0 = v[c], v1 = v[c + 1];
+                    if constexpr (EPI == EPI_GELU) {
+                        v0 += a.bias[c];
+                        v1 += a.bias[c + 1];
+                        pr[c / 2] = pack_bf16(v0, v1);
+                        o[c / 2] = pack_bf16(gelu(v0), gelu(v1));
+                    } else {
+                        const float g0 = gelu_grad(bf16_at(a.pre_in, p * N + c));
+                        const float g1 = gelu_grad(bf16_at(a.pre_in, p * N + c + 1));
+                        o[c / 2] = pack_bf16(v0 * g0, v1 * g1);
+                    }
+                }
+                uint4* dst = reinterpret_cast<uint4*>(static_cast<bf16*>(a.out) + p * N);
+#pragma unroll
+                for (int k = 0; k < N / 8; ++k)
+                    dst[k] = make_uint4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+                if constexpr (EPI == EPI_GELU) {
+                    if (a.pre_out) {
+                        uint4* dp = reinterpret_cast<uint4*>(a.pre_out + p * N);
+#pragma unroll
+                        for (int k = 0; k < N / 8; ++k)
+                            dp[k] = make_uint4(pr[4 * k], pr[4 * k + 1], pr[4 * k + 2], pr[4 * k + 3]);
+                    }
+                }
+            }
+        }
+    }
+    if (!ok && a.err) atomicOr(a.err, 1u);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) tmem_free(tmem, 2 * ACC_COLS);
+}
+
+template <int N, int EPI>
+cudaError_t launch_conv_tma(const ConvArgs& a, cudaStream_t s) {
+    CUtensorMap map;
+    if (reinterpret_cast<uintptr_t>(a.x) % 16 != 0 ||
+        !tensor_map_act_bf16(a.x, 32, a.W, a.H, a.B, 128, &map))
+        return cudaErrorNotSupported;
+    constexpr size_t smem = ct_smem_bytes<N>();
+    auto kern = conv_tma_kernel<N, EPI>;
+    static bool attr = false;
+    if (!attr) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const int xtiles = (a.W + 127) / 128;
+    const long long nt = (long long)xtiles * a.H * a.B;
+    if (nt >= (1ll << 31)) return cudaErrorInvalidValue;
+    const int grid = (int)std::min<long long>(nt, sm_count());
+    kern<<<grid, CT_THREADS, smem, s>>>(map, a, (int)nt, xtiles);
+    return cudaGetLastError();
+}
+
 template <int CIN, int N, int EPI>
 cudaError_t launch_conv(const ConvArgs& a, cudaStream_t s) {
     constexpr size_t smem = conv_smem_bytes<CIN, N>();
@@ -280,15 +475,21 @@ int lpbf_b200_sg_conv(int kind, const lpbf_b200_sg_conv_args* p, cudaStream_t st
             e = launch_conv<4, 32, EPI_GELU>(a, stream); break;
         case LPBF_SG_FWD_HIDDEN:
             if (!a.bias) return LPBF_ERR_ARG;
-            e = launch_conv<32, 32, EPI_GELU>(a, stream); break;
+            e = launch_conv_tma<32, EPI_GELU>(a, stream);
+            if (e == cudaErrorNotSupported) e = launch_conv<32, 32, EPI_GELU>(a, stream);
+            break;
         case LPBF_SG_FWD_OUT:
-            e = launch_conv<32, 16, EPI_LINEAR>(a, stream); break;
+            e = launch_conv_tma<16, EPI_LINEAR>(a, stream);
+            if (e == cudaErrorNotSupported) e = launch_conv<32, 16, EPI_LINEAR>(a, stream);
+            break;
         case LPBF_SG_DX_OUT:
             if (!a.pre_in) return LPBF_ERR_ARG;
             e = launch_conv<1, 32, EPI_DGELU>(a, stream); break;
         case LPBF_SG_DX_HIDDEN:
             if (!a.pre_in) return LPBF_ERR_ARG;
-            e = launch_conv<32, 32, EPI_DGELU>(a, stream); break;
+            e = launch_conv_tma<32, EPI_DGELU>(a, stream);
+            if (e == cudaErrorNotSupported) e = launch_conv<32, 32, EPI_DGELU>(a, stream);
+            break;
         default:
             return LPBF_ERR_ARG;
     }
