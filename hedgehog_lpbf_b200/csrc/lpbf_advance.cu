@@ -288,6 +288,7 @@ int lpbf_b200_advance_launches(int nx, int ny, int n_steps, const lpbf_b200_opts
 int lpbf_b200_advance(double* T_a, double* T_b, const StepConst* k, const lpbf_tick* plan,
                       int n_steps, const lpbf_b200_opts* opts, Partial* ring, void* work,
                       size_t work_bytes, cudaStream_t stream, int* result_in_b) {
+    NvtxRange nvtx_range("lpbf_b200_advance");
     if (!valid_const(k) || !opts || !T_a || !T_b || T_a == T_b || n_steps < 0 ||
         (n_steps > 0 && !plan) || !result_in_b)
         return LPBF_ERR_ARG;

@@ -330,7 +330,7 @@ struct WarpStrip {
             const int st = g % ADV_S;
             const bool ok = mbar_wait_bounded(&bars[st], (g / ADV_S) & 1);
             if (!__all_sync(0xffffffffu, ok)) {
-                if (lane == 0) atomicOr(p.err, 1u);
+                if (lane == 0 && p.err) atomicOr(p.err, 1u);
                 failed = true;
                 return nullptr;
             }
@@ -555,8 +555,10 @@ struct WarpStrip {
         bool rh = false;
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-            if (full) rh = rh | (nv[v] > thr[T]);
-            else      rh = rh | (own && xl + v < p.c.nx && nv[v] > thr[T]);
+            // !(v <= thr): the same test as v > thr for numbers, and true for
+            // NaN, so a non-finite cell reaches the exact pass (which flags it)
+            if (full) rh = rh | !(nv[v] <= thr[T]);
+            else      rh = rh | (own && xl + v < p.c.nx && !(nv[v] <= thr[T]));
         }
         hit[T] = hit[T] | rh;
         if constexpr (T == K - 1) {
@@ -591,6 +593,7 @@ struct WarpStrip {
         const int nx = p.c.nx;
         const bool ol = owned_lane();
         double m = -INFINITY;
+        bool nonfinite = false;
         for (int P = 0; P < 3; ++P) {
             const int r = j + P - t;
             const bool cand = r >= y0 && r < y1 && ol && (t < K || ((kmask >> P) & 1u));
@@ -602,12 +605,16 @@ struct WarpStrip {
                 if (ok) x = rs->box[P][lane][v];
                 m = (ok && x > m) ? x : m;
                 hot |= ok && x > p.c.Tm;
+                nonfinite |= ok && !(fabs(x) < INFINITY);
             }
             if (__any_sync(0xffffffffu, hot) && lane == 0) {
                 rs->ymn[t - 1] = min(rs->ymn[t - 1], r);
                 rs->ymx[t - 1] = max(rs->ymx[t - 1], r);
             }
         }
+        // a NaN or infinite temperature is reported, never trapped on; the
+        // peak keeps the reference rule (NaN never wins)
+        if (__any_sync(0xffffffffu, nonfinite) && lane == 0 && p.err) atomicOr(p.err, 2u);
         const double pk = rs->tmx[t - 1][lane];
         if (m > pk || (incl && m == pk)) {
             long long arg = -1;

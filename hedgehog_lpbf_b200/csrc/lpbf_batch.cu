@@ -529,6 +529,7 @@ size_t lpbf_b200_batch_workspace_bytes(const lpbf_b200_scenario* sc, int n_scen,
 int lpbf_b200_batch_create(const lpbf_b200_scenario* sc, int n_scen, int n_steps,
                            const lpbf_b200_batch_opts* opts, void* work, size_t work_bytes,
                            cudaStream_t stream, lpbf_b200_batch** out) {
+    NvtxRange nvtx_range("lpbf_b200_batch_create");
     if (!out) return LPBF_ERR_ARG;
     *out = nullptr;
     if (!sc || n_scen <= 0 || n_steps < 0 || !valid_opts(opts)) return LPBF_ERR_ARG;
@@ -672,6 +673,7 @@ extern "C" {
 
 int lpbf_b200_batch_run(lpbf_b200_batch* b, int first_step, int n_steps, int use_graph,
                         cudaStream_t stream) {
+    NvtxRange nvtx_range("lpbf_b200_batch_run");
     if (!valid_range(b, first_step, n_steps)) return LPBF_ERR_ARG;
     if (n_steps == 0) return LPBF_OK;
     int par = b->cur;
@@ -689,6 +691,7 @@ int lpbf_b200_batch_run(lpbf_b200_batch* b, int first_step, int n_steps, int use
 
 int lpbf_b200_batch_run_wsub(lpbf_b200_batch* b, int first_step, int n_steps,
                              const unsigned char* cruise, double* w_sub, cudaStream_t stream) {
+    NvtxRange nvtx_range("lpbf_b200_batch_run_wsub");
     if (!valid_range(b, first_step, n_steps) || !cruise || !w_sub || !b->all_rings)
         return LPBF_ERR_ARG;
     const BatchScen* scen = reinterpret_cast<const BatchScen*>(b->work + b->lay.off_scen);

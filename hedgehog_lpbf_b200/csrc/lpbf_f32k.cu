@@ -139,6 +139,7 @@ int lpbf_b200_advance_f32k(float* hi_a, float* lo_a, float* hi_b, float* lo_b,
                            const StepConst* k, const lpbf_tick* plan, int n_steps,
                            const lpbf_b200_opts* opts, Partial* ring, void* work,
                            size_t work_bytes, cudaStream_t stream, int* result_in_b) {
+    NvtxRange nvtx_range("lpbf_b200_advance_f32k");
     if (!k || k->nx < 2 || k->ny < 1 || !opts || !hi_a || !lo_a || !hi_b || !lo_b ||
         n_steps < 0 || (n_steps > 0 && !plan) || !result_in_b)
         return LPBF_ERR_ARG;

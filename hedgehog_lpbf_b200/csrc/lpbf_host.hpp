@@ -14,9 +14,20 @@
 #include <algorithm>
 #include <cmath>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "lpbf_device.cuh"
 
 namespace lpbf_b200 {
+
+// NVTX range over a host entry point (visible in Nsight timelines; a no-op
+// without a tool attached).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 constexpr int MAX_CTAS = 2048;     // most CTAs a reducing launch may use
 

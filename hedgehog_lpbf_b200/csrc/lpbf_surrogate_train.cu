@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "lpbf_host.hpp"
 #include "lpbf_surrogate.cuh"
 #include "lpbf_b200.h"
 
@@ -492,6 +493,7 @@ int lpbf_b200_sg_net_get(const void* net, float* params, float* grads, cudaStrea
 int lpbf_b200_sg_forward(const void* net, const void* x4, float* y, int batch, int height,
                          int width, void* work, size_t work_bytes, unsigned int* err,
                          cudaStream_t stream) {
+    NvtxRange nvtx_range("lpbf_b200_sg_forward");
     if (!net || !x4 || !y || batch < 1 || height < 1 || width < 1) return LPBF_ERR_ARG;
     const long long P = (long long)batch * height * width;
     Work w = work_layout(static_cast<unsigned char*>(work), P, false);
@@ -558,6 +560,7 @@ int lpbf_b200_sg_adamw(void* net, const lpbf_b200_sg_hyper* h, cudaStream_t stre
 int lpbf_b200_sg_train_step(void* net, const void* x4, const float* target, int batch, int height,
                             int width, const lpbf_b200_sg_hyper* h, void* work, size_t work_bytes,
                             float* loss, unsigned int* err, cudaStream_t stream) {
+    NvtxRange nvtx_range("lpbf_b200_sg_train_step");
     if (!h) return LPBF_ERR_ARG;
     const int st = lpbf_b200_sg_gradients(net, x4, target, batch, height, width, work, work_bytes,
                                           loss, err, stream);

@@ -307,6 +307,7 @@ int lpbf_b200_batch_tune_key(const lpbf_b200_scenario* sc, int n_scen, char* buf
 
 int lpbf_b200_batch_autotune(const lpbf_b200_scenario* sc, int n_scen, int n_steps,
                              const char* cache_path, int trial_steps, lpbf_b200_batch_opts* out) {
+    NvtxRange nvtx_range("lpbf_b200_batch_autotune");
     if (!sc || n_scen <= 0 || !out || trial_steps < 1 || n_steps < trial_steps)
         return LPBF_ERR_ARG;
     for (int i = 0; i < n_scen; ++i)

@@ -159,6 +159,17 @@ def _window(plan, s0, s1, k, margin, nx, ny):
     return max(0, y0), min(ny, y1 + 1), max(0, x0), min(nx, x1 + 1)
 
 
+def judge(got: torch.Tensor, ref: torch.Tensor, tol_K: float, area_tol: float, Tm: float):
+    """The FP64 judge's verdict on one window: (max |got - ref| in K, melt-pool
+    area error, roll back?).  Roll back where the field misses by more than
+    tol_K or the area of T > Tm differs by more than area_tol (relative)."""
+    diff = float((got - ref).abs().max().item())
+    a_ref = int((ref > Tm).sum().item())
+    a_got = int((got > Tm).sum().item())
+    area = abs(a_got - a_ref) / max(a_ref, 1) if (a_ref or a_got) else 0.0
+    return diff, area, (diff > tol_K or area > area_tol or not math.isfinite(diff))
+
+
 def run_hybrid(net: Net, k, plan, T0, n_steps: int, judge_every: int = 8, tol_K: float = 5.0,
                area_tol: float = 0.02, Tm: float = 1700.0, margin: int | None = None,
                halo: int = 32, device="cuda:0"):
@@ -194,20 +205,17 @@ def run_hybrid(net: Net, k, plan, T0, n_steps: int, judge_every: int = 8, tol_K:
         sub_plan = plan[s_blk:s_blk + STEPS * judge_every].copy()
         sub_plan["x_l"] -= hx0 * k.dx
         sub_plan["y_l"] -= hy0 * k.dy
-        judge = Solver(ks, Tm=Tm, device=dev, T0=Tw0.cpu().numpy())
-        judge.advance(sub_plan)
+        fp64 = Solver(ks, Tm=Tm, device=dev, T0=Tw0.cpu().numpy())
+        fp64.advance(sub_plan)
         iy0, iy1, ix0, ix1 = wy0 - hy0, wy1 - hy0, wx0 - hx0, wx1 - hx0
-        ref = judge.field[iy0:iy1, ix0:ix1]
+        ref = fp64.field[iy0:iy1, ix0:ix1]
         got = T[wy0:wy1, wx0:wx1]
-        diff = float((got - ref).abs().max().item())
-        a_ref = int((ref > Tm).sum().item())
-        a_got = int((got > Tm).sum().item())
-        area = abs(a_got - a_ref) / max(a_ref, 1) if (a_ref or a_got) else 0.0
+        diff, area, back = judge(got, ref, tol_K, area_tol, Tm)
         rec["judged"] += 1
         rec["fp64_window_cells"] += (hy1 - hy0) * (hx1 - hx0)
         rec["worst_K"] = max(rec["worst_K"], diff)
         rec["worst_area"] = max(rec["worst_area"], area)
-        if diff > tol_K or area > area_tol:
+        if back:
             T[wy0:wy1, wx0:wx1] = ref
             rec["rolled_back"] += 1
     e1.record()

@@ -92,7 +92,10 @@ int lpbf_b200_advance(double* T_a, double* T_b, const StepConst* k,
 int lpbf_b200_advance_launches(int nx, int ny, int n_steps, const lpbf_b200_opts* opts);
 
 /* Copy the workspace error word to *err (synchronizes `stream`); bit 0 means
- * a TMA wait exceeded its time limit and the launch stopped early. */
+ * a TMA wait exceeded its time limit and the launch stopped early; bit 1
+ * means a computed temperature was NaN or infinite (baseline FP64 advance
+ * with a ring; the Partials ignore NaN as the reference does).  The word
+ * accumulates until lpbf_b200_workspace_init clears it. */
 int lpbf_b200_read_error(const void* work, cudaStream_t stream, unsigned int* err);
 
 /* FP32 compensated variant (no reference counterpart; the reference path is
@@ -209,7 +212,8 @@ int lpbf_b200_batch_launches(const lpbf_b200_batch* b, int n_steps);
 int lpbf_b200_batch_tasks(const lpbf_b200_batch* b);
 int lpbf_b200_batch_scenario_rows(const lpbf_b200_batch* b, int scenario);
 /* Error word (synchronizes `stream`): bit 0 = a copy wait exceeded its time
- * limit; the batch's counters are then undefined: destroy and re-create it. */
+ * limit (the batch's counters are then undefined: destroy and re-create it);
+ * bit 1 = a scenario computed a NaN or infinite temperature. */
 int lpbf_b200_batch_read_error(const lpbf_b200_batch* b, cudaStream_t stream, unsigned int* err);
 /* Frees the host object and its graphs; the workspace is the caller's again. */
 void lpbf_b200_batch_destroy(lpbf_b200_batch* b);

@@ -190,3 +190,26 @@ def test_autotune_trials_cache_and_tuned_batch(gpu, tmp_path):
     b.run(0, n, use_graph=True)
     _assert_same(b, scs, n, refs)
     b.close()
+
+
+def test_snapshot_resume_is_bit_identical(gpu, tmp_path):
+    """(snapshot, step) is a full checkpoint: stopping after step s, writing
+    T_step_s.bin and resuming from it gives the uninterrupted run's field and
+    Partials bit for bit."""
+    from hedgehog_lpbf_b200 import checkpoint
+    from hedgehog_lpbf_b200.solver import Solver, ring_to_numpy
+    mat, dom, k = _const(600, 400)
+    n = 40
+    plan = PL.raster_for_steps(dom, k.dt, n, V=1.5, hatch=100e-6, n_tracks=2, angle=0.3)
+    a = Solver(k, Tm=mat.Tm, device="cuda:0")
+    ra = a.new_ring(n)
+    a.advance(plan, ra)
+    b = Solver(k, Tm=mat.Tm, device="cuda:0")
+    rb1 = b.new_ring(17)
+    b.advance(plan[:17], rb1)
+    checkpoint.save(b.field, str(tmp_path), 16)
+    c = checkpoint.resume(Solver(k, Tm=mat.Tm, device="cuda:0"), str(tmp_path), 16)
+    rb2 = c.new_ring(n - 17)
+    c.advance(plan[17:], rb2)
+    assert np.array_equal(c.field.cpu().numpy().view(np.uint64), a.field.cpu().numpy().view(np.uint64))
+    assert (ring_to_numpy(rb1).tobytes() + ring_to_numpy(rb2).tobytes()) == ring_to_numpy(ra).tobytes()

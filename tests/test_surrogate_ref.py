@@ -49,3 +49,38 @@ def test_adamw_first_step_is_sign_like():
     p1, m, v = R.adamw(p, g, np.zeros(3), np.zeros(3), 1, lr=1e-2, wd=0.0)
     assert np.allclose(p1[:2], p[:2] - 1e-2 * np.sign(g[:2]), atol=1e-7)
     assert p1[2] == p[2]
+
+
+def test_judge_gates_with_host_side_fault_injection():
+    """The rollback gates of the in-loop judge on CPU tensors: a window that
+    matches passes; 6 K off at one cell, a 3 % melt-area change, or a NaN
+    roll back; 4 K off with the same melt area does not."""
+    import torch
+    from hedgehog_lpbf_b200.superstep import judge
+    rng = np.random.default_rng(0)
+    ref = torch.tensor(300.0 + 1700.0 * rng.random((64, 80)))
+    Tm = 1700.0
+    assert judge(ref.clone(), ref, 5.0, 0.02, Tm)[2] is False
+    got = ref.clone()
+    cool = int(torch.nonzero(ref < Tm - 50)[0][0]), int(torch.nonzero(ref < Tm - 50)[0][1])
+    got[cool] += 4.0
+    d, a, back = judge(got, ref, 5.0, 0.02, Tm)
+    assert abs(d - 4.0) < 1e-9 and a == 0.0 and back is False
+    got[cool] += 2.0
+    assert judge(got, ref, 5.0, 0.02, Tm)[2] is True
+    # melt area: push 3 % of the molten cells below Tm by a little (< 5 K)
+    got = ref.clone()
+    hot = torch.nonzero((ref > Tm) & (ref < Tm + 2.0))
+    molten = int((ref > Tm).sum())
+    need = int(np.ceil(0.03 * molten))
+    if len(hot) < need:                      # make enough cells sit just above Tm
+        flat = torch.nonzero(ref > Tm)[:need]
+        ref[flat[:, 0], flat[:, 1]] = Tm + 1.0
+        got = ref.clone()
+        hot = flat
+    got[hot[:need, 0], hot[:need, 1]] = Tm - 1.0
+    d, a, back = judge(got, ref, 5.0, 0.02, Tm)
+    assert d <= 5.0 and a >= 0.03 and back is True
+    got = ref.clone()
+    got[0, 0] = float("nan")
+    assert judge(got, ref, 5.0, 0.02, Tm)[2] is True

@@ -82,3 +82,28 @@ def test_batch_ties(gpu):
         for i in range(len(scs)):
             _check(b.ring(i), refs[i], n)
         b.close()
+
+
+@pytest.mark.parametrize("bad", [float("nan"), float("inf")])
+def test_non_finite_cells_are_flagged_not_trapped(gpu, bad):
+    """A NaN or infinite temperature sets bit 1 of the error word; the
+    per-step Partials keep the reference rule (NaN never wins, +inf does)."""
+    from hedgehog_lpbf_b200.solver import Solver, ring_to_numpy
+    n = 5
+    mat, dom, k = _const(400, 300)
+    plan = _plan(dom, k, n, True)
+    T0 = np.full((300, 400), 300.0)
+    T0[150, 200] = bad
+    s = Solver(k, Tm=1400.0, depth=3, device="cuda:0", T0=T0)
+    assert s.read_error() == 0
+    ring = s.new_ring(n)
+    s.advance(plan, ring)
+    assert s.read_error() & 2
+    _, ring_ref = O.run(T0.ravel(), k, PL.laser_array(plan), Tm=1400.0)
+    r = ring_to_numpy(ring)
+    assert np.array_equal(r["arg"], ring_ref["arg"])
+    assert np.array_equal(r["tmax"], ring_ref["tmax"]) or np.allclose(
+        r["tmax"], ring_ref["tmax"], rtol=1e-12)
+    clean = Solver(k, Tm=1400.0, depth=3, device="cuda:0")
+    clean.advance(plan, clean.new_ring(n))
+    assert clean.read_error() == 0
