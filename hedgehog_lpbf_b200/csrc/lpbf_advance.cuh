@@ -276,6 +276,8 @@ struct WarpStrip {
             }
         }
         const int jlast = y1 - 1 + K;
+        // per-box thresholds change only when an exact pass moves a peak
+        if constexpr (REDUCE) set_thresholds();
         for (int b = 0, j = jy0; j <= jlast && !failed; ++b, j += ADV_R) {
             const double* st = nullptr;
             if (j < jend) {
@@ -283,7 +285,6 @@ struct WarpStrip {
                 if (failed) break;
             }
             // computed rows of this box: j-K .. j+1 over all levels
-            if constexpr (REDUCE) set_thresholds();
             const bool fast = !edge && j - K >= 1 && j + 1 <= ny - 2 && p.st256 &&
                               (!src_strip || j + 1 < p.band_lo || j - K > p.band_hi);
             if (fast && j < jend) {
@@ -661,6 +662,7 @@ struct WarpStrip {
             exact_level(t, j);
         }
         __syncwarp();
+        set_thresholds();
     }
 };
 
