@@ -176,6 +176,14 @@ struct WarpStrip {
     int x0, xs, xl, y0, y1, jy0, jend, nbox, issued;
     int last_chunk;                      // row chunk of this warp's previous task (-1: none)
     bool edge, failed, own_all, src_strip;
+    // Mirror-edge strips on the fast body: the lane just off the field
+    // (columns -4..-1, or nx..nx+3) holds the reversed cells of its field
+    // neighbour, so the field's edge cell sees itself as its outer neighbour
+    // through the ordinary shuffle.
+    bool mir;                            // this task keeps mirror lanes (warp-uniform)
+    bool mlane;                          // this lane is a mirror lane
+    int msrc;                            // lane whose cells this lane mirrors (own lane if none)
+    bool fast_ok;                        // the task may use the fast body at all
     bool incl;                           // this task also examines values equal to the lane peak
 
     double w0[3][V];                     // level-0 window (slot = row % 3)
@@ -266,7 +274,13 @@ struct WarpStrip {
         jend = min(y1 + K, ny);
         nbox = (jend - jy0 + ADV_R - 1) / ADV_R;
         edge = (xs <= 0) || (xs + ADV_COLS > nx - 1);
-        own_all = lane >= 1 && lane <= 30;
+        own_all = owned_lane();
+        // With nx a multiple of 4 every lane lies wholly on or off the field;
+        // the mirror lanes are the lane before column 0 and the lane at nx.
+        mir = edge && p.st256 && p.c.bc == 0;
+        mlane = mir && (xl == -V || xl == nx);
+        msrc = !mlane ? lane : (xl < 0 ? lane + 1 : lane - 1);
+        fast_ok = (!edge || mir) && p.st256 && p.c.same_T;
         src_strip = !(xs + ADV_COLS <= p.bandx_lo || xs > p.bandx_hi);
         issued = 0;
         if constexpr (TMA) {
@@ -285,7 +299,7 @@ struct WarpStrip {
                 if (failed) break;
             }
             // computed rows of this box: j-K .. j+1 over all levels
-            const bool fast = !edge && j - K >= 1 && j + 1 <= ny - 2 && p.st256 &&
+            const bool fast = fast_ok && j - K >= 1 && j + 1 <= ny - 2 &&
                               (!src_strip || j + 1 < p.band_lo || j - K > p.band_hi);
             if (fast && j < jend) {
                 fast_row<0>(j, st);
@@ -374,9 +388,22 @@ struct WarpStrip {
     }
 
     // ---- fast body -------------------------------------------------------
+    // A mirror lane takes its neighbour lane's cells in reverse order (the
+    // mirror image about the field edge); other lanes keep theirs.
+    __device__ __forceinline__ void mirror_fix(double* v) {
+        double m[V];
+#pragma unroll
+        for (int i = 0; i < V; ++i) m[i] = __shfl_sync(0xffffffffu, v[i], msrc);
+        if (mlane) {
+#pragma unroll
+            for (int i = 0; i < V; ++i) v[i] = m[V - 1 - i];
+        }
+    }
+
     template <int P>
     __device__ __forceinline__ void fast_row(int jj, const double* st) {
         load_row0<P>(jj, st, win<0>()[P]);
+        if (mir) mirror_fix(win<0>()[P]);
         fast_level<P, 1>(jj);
     }
 
@@ -415,7 +442,10 @@ struct WarpStrip {
     template <int P>
     __device__ __forceinline__ void general_row(int jj, const double* st, int jlast) {
         if (jj > jlast) return;
-        if (jj < jend) load_row0<P>(jj, st, win<0>()[P]);
+        if (jj < jend) {
+            load_row0<P>(jj, st, win<0>()[P]);
+            if (mir) mirror_fix(win<0>()[P]);
+        }
         general_level<P, 1>(jj);
     }
 
@@ -442,6 +472,11 @@ struct WarpStrip {
                 }
                 double nv[V];
                 compute_row_general(wn[su], wn[sc], wn[sd], r, p.las[T - 1], nv);
+                // keep the mirror lanes exact for later fast boxes (the source
+                // term and the edge patch are not mirror-symmetric off the field)
+                if constexpr (T < K) {
+                    if (mir) mirror_fix(nv);
+                }
                 const bool owned_row = r >= y0 && r < y1;
                 if constexpr (T < K) {
                     double (&wo)[3][V] = win<T>();

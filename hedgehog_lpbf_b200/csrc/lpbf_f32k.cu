@@ -19,9 +19,15 @@ FkCoef make_fk(const Coef& c, double T_edge) {
     f.ay = (float)c.ay;
     f.cls = (float)c.c_ls;
     f.crad = (float)c.c_rad;
-    f.Ta_hi = (float)c.Tamb;
-    f.Ta_lo = (float)(c.Tamb - (double)f.Ta_hi);
-    f.Ta4 = fk_pow4(f.Ta_hi, f.Ta_lo);
+    // radiation is referred to Tamb; the linear losses to the temperature
+    // at which convection (Tamb) and substrate conduction (Tsub) cancel:
+    // c_conv (T - Tamb) + c_sub (T - Tsub) = c_ls (T - Tlin)
+    const float a_hi = (float)c.Tamb;
+    f.Ta4 = fk_pow4(a_hi, (float)(c.Tamb - (double)a_hi));
+    const double Tlin = (c.same_T || c.c_ls == 0.0)
+                            ? c.Tamb : (c.c_conv * c.Tamb + c.c_sub * c.Tsub) / c.c_ls;
+    f.Ta_hi = (float)Tlin;
+    f.Ta_lo = (float)(Tlin - (double)f.Ta_hi);
     f.Tedge_hi = (float)T_edge;
     f.Tedge_lo = (float)(T_edge - (double)f.Tedge_hi);
     return f;

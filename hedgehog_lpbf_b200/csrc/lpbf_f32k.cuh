@@ -33,7 +33,7 @@ constexpr size_t FK_SMEM_BYTES =
 
 struct FkCoef {
     float ax, ay, cls, crad;
-    float Ta_hi, Ta_lo, Ta4;       // Tamb as a pair; Ta4 = f4(Ta_hi + Ta_lo)
+    float Ta_hi, Ta_lo, Ta4;       // linear-loss reference T as a pair; Ta4 = f4(Tamb)
     float Tedge_hi, Tedge_lo;
 };
 

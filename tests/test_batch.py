@@ -139,19 +139,23 @@ def test_batch_matches_oracle_small(gpu):
     from oracle import oracle as O
     from hedgehog_lpbf_b200.batch import Batch, batch_opts
     n = 9
-    scs = _mixed(n, [(120, 90, 0), (200, 64, 1)], seed=8)
-    b = Batch(scs, n, opts=batch_opts(depth=4), device="cuda:0")
-    b.run(0, n)
-    for i, sc in enumerate(scs):
-        T_ref, ring_ref = O.run(np.asarray(sc.T0).ravel(), sc.k, PL.laser_array(sc.plan[:n]),
-                                bc=sc.bc, T_D=sc.T_edge, Tm=sc.Tm)
-        T = b.field(i).cpu().numpy().ravel()
-        err = float(np.max(np.abs(T - T_ref) / np.maximum(np.abs(T_ref), 1.0)))
-        assert err <= 1e-12, err
-        r = b.ring(i)
-        assert np.array_equal(r["arg"], ring_ref["arg"])
-        assert np.max(np.abs(r["tmax"] - ring_ref["tmax"]) / ring_ref["tmax"]) <= 1e-12
-    b.close()
+    # mirror edges mid-strip (248 = 2 strips + 8 columns), a substrate
+    # temperature other than the ambient one, fixed edges
+    scs = _mixed(n, [(120, 90, 0), (200, 64, 1), (248, 96, 0), (244, 80, 0)], seed=8)
+    scs[3].k.Tsub = 420.0
+    refs = [O.run(np.asarray(sc.T0).ravel(), sc.k, PL.laser_array(sc.plan[:n]),
+                  bc=sc.bc, T_D=sc.T_edge, Tm=sc.Tm) for sc in scs]
+    for staging in (1, 2):
+        b = Batch(scs, n, opts=batch_opts(depth=4, staging=staging), device="cuda:0")
+        b.run(0, n)
+        for i, (T_ref, ring_ref) in enumerate(refs):
+            T = b.field(i).cpu().numpy().ravel()
+            err = float(np.max(np.abs(T - T_ref) / np.maximum(np.abs(T_ref), 1.0)))
+            assert err <= 1e-12, (staging, i, err)
+            r = b.ring(i)
+            assert np.array_equal(r["arg"], ring_ref["arg"])
+            assert np.max(np.abs(r["tmax"] - ring_ref["tmax"]) / ring_ref["tmax"]) <= 1e-12
+        b.close()
 
 
 def test_batch_rejects_bad_arguments(gpu):

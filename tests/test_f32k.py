@@ -100,3 +100,16 @@ def test_f32k_split_join_round_trip(gpu):
     torch.cuda.synchronize()
     y = out.cpu().numpy()
     assert np.max(np.abs(y - x) / x) < 2.0 ** -46     # two f32 halves keep ~48 bits
+
+
+def test_f32k_substrate_temperature_differs_from_ambient(gpu):
+    mat, pr = P.benchmark_material_process()
+    pr.Tsub = 420.0
+    dom = P.Domain(Lx=299 * 5e-6, Ly=259 * 5e-6, nx=300, ny=260)
+    k = P.make_const(mat, pr, dom, P.dt_fraction(mat, dom))
+    T0 = np.full(300 * 260, 300.0)
+    plan = PL.raster_for_steps(dom, k.dt, 400, V=1.0, hatch=100e-6, n_tracks=2)
+    T_ref, ring_ref = O.run(T0, k, PL.laser_array(plan), Tm=mat.Tm)
+    T, ring, _ = _run_f32k(k, plan, T0, Tm=mat.Tm)
+    assert float(np.max(np.abs(T - T_ref))) <= ATOL_K
+    assert float(np.max(np.abs(ring["tmax"] - ring_ref["tmax"]))) <= ATOL_K

@@ -275,3 +275,63 @@ def test_cuda_graph_capture_replays_advance(gpu):
     s.cur = 1 - start if eager.launches(16) % 2 else start
     assert np.array_equal(s.field.cpu().numpy(), eager.field.cpu().numpy())
     assert ring_to_numpy(ring).tobytes() == ring_to_numpy(r_e).tobytes()
+
+
+def _const_tsub(nx, ny, Tsub):
+    mat, pr = P.benchmark_material_process()
+    pr.Tsub = Tsub
+    dom = P.Domain(Lx=(nx - 1) * 5e-6, Ly=(ny - 1) * 5e-6, nx=nx, ny=ny)
+    return mat, pr, dom, P.make_const(mat, pr, dom, P.dt_fraction(mat, dom))
+
+
+@pytest.mark.parametrize("bc", [0, 1])
+def test_substrate_temperature_differs_from_ambient(gpu, bc):
+    """Tsub != Tamb: convection and substrate conduction pull towards different
+    temperatures, so the two linear loss terms stay separate (the reference's
+    q_top / q_bot)."""
+    from hedgehog_lpbf_b200.solver import ring_to_numpy
+    nx, ny = 300, 260
+    mat, pr, dom, k = _const_tsub(nx, ny, 420.0)
+    rng = np.random.default_rng(21)
+    T0 = 300.0 + rng.uniform(0.0, 1500.0, size=nx * ny)
+    n = 9
+    plan = PL.raster_for_steps(dom, k.dt, n, V=1.0, hatch=100e-6, n_tracks=2, angle=0.4)
+    T_ref, ring_ref = O.run(T0, k, PL.laser_array(plan), bc=bc, T_D=300.0, Tm=mat.Tm)
+    for depth in (1, 3, 4):
+        s = solver(k, bc=bc, T_edge=300.0, Tm=mat.Tm, depth=depth, T0=T0)
+        ring = s.new_ring(n)
+        T = s.advance(plan, ring).cpu().numpy()
+        assert rel_err(T, T_ref) <= RTOL, depth
+        check_partials(ring_to_numpy(ring), ring_ref, T_ref, nx)
+
+
+@pytest.mark.parametrize("nx", [4, 8, 116, 120, 124, 128, 244, 248, 252, 364])
+def test_mirror_edge_strips(gpu, nx):
+    """Mirror edges on the fast body: for every position of the right edge
+    inside a strip (the lane past the field anywhere from lane 1 to beyond
+    the strip) and fields narrower than one strip, with the laser crossing
+    both side edges, depths 1..4 agree bit for bit and match the oracle."""
+    from hedgehog_lpbf_b200.solver import ring_to_numpy
+    ny = 90
+    mat, pr, dom, k = bench_const(nx, ny)
+    rng = np.random.default_rng(nx)
+    T0 = 300.0 + rng.uniform(0.0, 1500.0, size=nx * ny)
+    n = 10
+    xs = np.linspace(-0.05, 1.05, n) * dom.Lx
+    las = np.stack([xs, np.linspace(0.3, 0.7, n) * dom.Ly, np.ones(n)], axis=1)
+    plan = tick_plan(las)
+    T_ref, ring_ref = O.run(T0, k, las, Tm=mat.Tm)
+    first = None
+    for depth in (1, 2, 3, 4):
+        for rows in (0, 8):
+            s = solver(k, Tm=mat.Tm, depth=depth, rows=rows, T0=T0)
+            ring = s.new_ring(n)
+            T = s.advance(plan, ring).cpu().numpy()
+            r = ring_to_numpy(ring)
+            if first is None:
+                first = (T, r)
+                assert rel_err(T, T_ref) <= RTOL
+                check_partials(r, ring_ref, T_ref, nx)
+            else:
+                assert np.array_equal(T.view(np.uint64), first[0].view(np.uint64)), (depth, rows)
+                assert r.tobytes() == first[1].tobytes(), (depth, rows)
