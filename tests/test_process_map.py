@@ -5,6 +5,7 @@ import math
 import subprocess
 
 import numpy as np
+import pytest
 
 from hedgehog_lpbf_b200 import _lib
 from hedgehog_lpbf_b200 import process_map as PM
@@ -120,3 +121,25 @@ def test_tune_key_is_the_size_class_histogram():
         counts[_lib.lib().lpbf_b200_batch_size_class(s.k.nx, s.k.ny)] += 1
     pow2 = [0 if c == 0 else 1 << (c - 1).bit_length() for c in counts]
     assert key.endswith("classes " + ",".join(map(str, pow2)))
+
+
+def test_summarize_melt_results():
+    from hedgehog_lpbf_b200.solver import PARTIAL_DTYPE
+    r = np.zeros(5, dtype=PARTIAL_DTYPE)
+    r["tmax"] = [400.0, 1800.0, 2100.0, 1650.0, 1200.0]
+    r["ymin"] = [90, 40, 38, 45, 90]
+    r["ymax"] = [-1, 44, 47, 46, -1]
+    s = PM.summarize(r, 5e-6)
+    assert s["peak_T_K"] == 2100.0 and s["peak_step"] == 2
+    assert s["first_melt_step"] == 1 and s["molten_steps"] == 3
+    assert s["max_melt_rows"] == 10 and abs(s["max_melt_extent_um"] - 50.0) < 1e-9
+    none = np.zeros(2, dtype=PARTIAL_DTYPE)
+    none["ymax"] = -1
+    assert PM.summarize(none, 5e-6)["first_melt_step"] == -1
+
+
+def test_process_map_cli_rejects_bad_arguments():
+    with pytest.raises(SystemExit):
+        PM.main(["--scenarios", "0"])
+    with pytest.raises(SystemExit):
+        PM.main(["--rows", "1,2", "--depth", "2", "--steps", "0"])
