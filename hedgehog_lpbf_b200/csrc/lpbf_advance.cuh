@@ -433,7 +433,13 @@ struct WarpStrip {
             } else {
                 st_global_v4_pred(p.Tout + (size_t)r * p.c.nx + xl, nv, owned_row && own_all);
             }
-            if constexpr (REDUCE) row_stats<T - 1, P>(r, nv, own_all && owned_row, true);
+            // Only owned rows are tested: the first halo rows of a task are
+            // computed from window slots that still hold the warp's previous
+            // task (values of no use here, which would only trigger empty
+            // exact passes).
+            if constexpr (REDUCE) {
+                if (owned_row) row_stats<T - 1, P>(r, nv, own_all, true);
+            }
             fast_level<P, T + 1>(jj);
         }
     }
@@ -485,7 +491,9 @@ struct WarpStrip {
                 } else {
                     if (owned_row) store_row(r, nv);
                 }
-                if constexpr (REDUCE) row_stats<T - 1, P>(r, nv, owned_row && owned_lane(), !edge);
+                if constexpr (REDUCE) {
+                    if (owned_row) row_stats<T - 1, P>(r, nv, owned_lane(), !edge);
+                }
             }
             general_level<P, T + 1>(jj);
         }
@@ -607,67 +615,66 @@ struct WarpStrip {
         }
     }
 
-    // Copy level T's three box rows (slots of rows j-T .. j-T+2) to shared memory.
+    // Exact update of level T (1..K) from three of its rows (row j + P - T
+    // in x[P]; only rows set in `rows` take part): the lane's first maximal
+    // owned cell in flat-index order, the molten-row extent, non-finite
+    // cells.  Each lane reads only its own values, so no warp barrier is
+    // needed around the scan.
     template <int T>
-    __device__ __forceinline__ void stage_level() {
-        if constexpr (T >= 1 && T < K) {
-            const double (&wn)[3][V] = win<T>();
-#pragma unroll
-            for (int P = 0; P < 3; ++P) {
-                double2* d = reinterpret_cast<double2*>(&rs->box[P][lane][0]);
-                d[0] = make_double2(wn[mod3(P - T)][0], wn[mod3(P - T)][1]);
-                d[1] = make_double2(wn[mod3(P - T)][2], wn[mod3(P - T)][3]);
-            }
-        }
-    }
-
-    // Exact update of level t (1..K) from the box starting at row j, whose
-    // level-t rows are staged in rs->box: all three for t < K, the rows of
-    // kmask for t == K (the others crossed no threshold: every value there is
-    // at most the lane's peak so far and none is molten).
-    __device__ __forceinline__ void exact_level(int t, int j) {
+    __device__ __forceinline__ void exact_rows(const double (&x)[3][V], int j, unsigned rows) {
         const int nx = p.c.nx;
         const bool ol = owned_lane();
         double m = -INFINITY;
+        long long a = -1;
         bool nonfinite = false;
+#pragma unroll
         for (int P = 0; P < 3; ++P) {
-            const int r = j + P - t;
-            const bool cand = r >= y0 && r < y1 && ol && (t < K || ((kmask >> P) & 1u));
+            const int r = j + P - T;
+            const bool cand = ((rows >> P) & 1u) && r >= y0 && r < y1 && ol;
             bool hot = false;
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 const bool ok = cand && xl + v < nx;
-                double x = 0.0;
-                if (ok) x = rs->box[P][lane][v];
-                m = (ok && x > m) ? x : m;
-                hot |= ok && x > p.c.Tm;
-                nonfinite |= ok && !(fabs(x) < INFINITY);
+                const double val = x[P][v];
+                // rows, then columns, ascend: the first maximum has the
+                // smallest flat index (NaN never wins)
+                const bool take = ok && val > m;
+                m = take ? val : m;
+                a = take ? (long long)r * nx + xl + v : a;
+                hot |= ok && val > p.c.Tm;
+                nonfinite |= ok && !(fabs(val) < INFINITY);
             }
             if (__any_sync(0xffffffffu, hot) && lane == 0) {
-                rs->ymn[t - 1] = min(rs->ymn[t - 1], r);
-                rs->ymx[t - 1] = max(rs->ymx[t - 1], r);
+                rs->ymn[T - 1] = min(rs->ymn[T - 1], r);
+                rs->ymx[T - 1] = max(rs->ymx[T - 1], r);
             }
         }
         // a NaN or infinite temperature is reported, never trapped on; the
         // peak keeps the reference rule (NaN never wins)
         if (__any_sync(0xffffffffu, nonfinite) && lane == 0 && p.err) atomicOr(p.err, 2u);
-        const double pk = rs->tmx[t - 1][lane];
-        if (m > pk || (incl && m == pk)) {
-            long long arg = -1;
-            for (int P = 0; P < 3 && arg < 0; ++P) {
-                const int r = j + P - t;
-                if (!(r >= y0 && r < y1 && ol && (t < K || ((kmask >> P) & 1u)))) continue;
-                for (int v = 0; v < V; ++v) {
-                    if (xl + v >= nx) break;
-                    const double x = rs->box[P][lane][v];
-                    if (x == m) { arg = (long long)r * nx + xl + v; break; }
-                }
+        const double pk = rs->tmx[T - 1][lane];
+        // an equal peak (inclusive task) moves only to a smaller index
+        if (m > pk || (incl && m == pk && a < rs->arg[T - 1][lane])) {
+            rs->tmx[T - 1][lane] = m;
+            rs->arg[T - 1][lane] = a;
+        }
+    }
+
+    // Levels 1..K-1 straight from their register windows (the box's three
+    // rows of level T sit in slots mod3(P - T)).
+    template <int T>
+    __device__ __forceinline__ void resolve_levels(unsigned bits, int j) {
+        if constexpr (T < K) {
+            if ((bits >> (T - 1)) & 1u) {
+                const double (&wn)[3][V] = win<T>();
+                double x[3][V];
+#pragma unroll
+                for (int P = 0; P < 3; ++P)
+#pragma unroll
+                    for (int v = 0; v < V; ++v) x[P][v] = wn[mod3(P - T)][v];
+                exact_rows<T>(x, j, 7u);
             }
-            // an equal peak (inclusive task) moves only to a smaller index
-            if (m > pk || arg < rs->arg[t - 1][lane]) {
-                rs->tmx[t - 1][lane] = m;
-                rs->arg[t - 1][lane] = arg;
-            }
+            resolve_levels<T + 1>(bits, j);
         }
     }
 
@@ -680,29 +687,32 @@ struct WarpStrip {
         }
         bits = __reduce_or_sync(0xffffffffu, bits);
         if (bits == 0u) { kmask = 0u; return; }
-        // the last level first: its rows already sit in the staging area,
-        // which the other levels then reuse
-        if ((bits >> (K - 1)) & 1u) exact_level(K, j);
-        kmask = 0u;
-        for (int t = 1; t < K; ++t) {
-            if (!((bits >> (t - 1)) & 1u)) continue;
-            __syncwarp();
-            switch (t) {               // stage level t's rows from its registers
-                case 1: stage_level<1>(); break;
-                case 2: stage_level<2>(); break;
-                case 3: stage_level<3>(); break;
-                default: break;
+        // the last level from the rows that row_stats staged (those of kmask:
+        // the others crossed no threshold, so every value there is at most
+        // the lane's peak so far and none is molten)
+        if ((bits >> (K - 1)) & 1u) {
+            double x[3][V];
+#pragma unroll
+            for (int P = 0; P < 3; ++P) {
+                const double2* b = reinterpret_cast<const double2*>(&rs->box[P][lane][0]);
+                const double2 u = b[0], w2 = b[1];
+                x[P][0] = u.x; x[P][1] = u.y; x[P][2] = w2.x; x[P][3] = w2.y;
             }
-            __syncwarp();
-            exact_level(t, j);
+            exact_rows<K>(x, j, kmask);
         }
+        kmask = 0u;
+        resolve_levels<1>(bits, j);
         __syncwarp();
         set_thresholds();
     }
 };
 
+// Resident CTAs per SM the register budget is sized for.  The staged kernels
+// hold 48 KB of stages plus 15-21 KB of reduction state per CTA, so shared
+// memory admits three CTAs whatever K is; a tighter register cap would only
+// spill.
 template <int K>
-struct AdvOcc { static constexpr int min_ctas = (K <= 2) ? 4 : 3; };
+struct AdvOcc { static constexpr int min_ctas = 3; };
 
 template <int K, bool TMA, bool REDUCE>
 __global__ void __launch_bounds__(ADV_WARPS * 32, AdvOcc<K>::min_ctas)
