@@ -73,8 +73,8 @@ def measured_peaks():
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback (no MEASURED_PEAKS.json: earlier copy-bandwidth measurement on B200)"
 
 
 def profile_traffic(depth):
@@ -360,6 +360,8 @@ def superstep_leg(args, dev):
             peak = json.load(f).get("bf16_tflops")
     if peak:
         out["forward_4096sq"]["frac_of_measured_bf16"] = out["forward_4096sq"]["tflops"] / peak
+    else:   # earlier cuBLAS bf16 burst measurement on B200
+        out["forward_4096sq"]["frac_of_fallback_bf16_1590"] = out["forward_4096sq"]["tflops"] / 1590.0
     return out
 
 
@@ -484,7 +486,7 @@ def run_b200_arm(args, rank, world, local_rank):
         "config": config(depth, world),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
+                     "peak_source": peak_src,
                      "kernel": f"advance_kernel<{depth},TMA,reduce>",
                      "algorithmic_bytes": f"{BYTES_PER_UPDATE} B per cell-update x {cells} cells"
                                           f" x {steps_per_launch:g} steps per launch",
