@@ -28,6 +28,12 @@ class Opts(ctypes.Structure):
                 ("Tm", ctypes.c_double), ("depth", ctypes.c_int), ("rows", ctypes.c_int)]
 
 
+class Rows(ctypes.Structure):
+    """lpbf_b200_rows (include/lpbf_b200.h): a row strip of a larger field."""
+    _fields_ = [("row0", ctypes.c_int), ("global_ny", ctypes.c_int), ("lo", ctypes.c_int),
+                ("hi", ctypes.c_int)]
+
+
 class Scenario(ctypes.Structure):
     """lpbf_b200_scenario (include/lpbf_b200.h)."""
     _fields_ = [("k", ctypes.POINTER(StepConst)), ("plan", _vp), ("T_a", _vp), ("T_b", _vp),
@@ -78,6 +84,10 @@ SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_int)]),
     "lpbf_b200_advance_launches": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                   ctypes.POINTER(Opts)]),
+    "lpbf_b200_advance_rows": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(StepConst), _vp,
+                                              ctypes.c_int, ctypes.POINTER(Opts),
+                                              ctypes.POINTER(Rows), _vp, _vp, ctypes.c_size_t,
+                                              _vp]),
     "lpbf_b200_read_error": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_uint)]),
     "lpbf_b200_advance_f32k": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.POINTER(StepConst), _vp,
                                               ctypes.c_int, ctypes.POINTER(Opts), _vp, _vp,

@@ -124,7 +124,7 @@ namespace {
 template <int K, bool TMA, bool REDUCE>
 cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const LaserSub* las,
                      Partial* ring, Workspace* ws, Partial* ref_out, long long ref_nparts,
-                     int rows, cudaStream_t stream) {
+                     int rows, cudaStream_t stream, const RowWindow* win) {
     auto kern = advance_kernel<K, TMA, REDUCE>;
     const size_t smem = TMA ? ADV_SMEM_BYTES : 0;
 
@@ -150,7 +150,21 @@ cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const Laser
     std::memset(&p, 0, sizeof(p));
     p.c = c;
     for (int t = 0; t < K; ++t) p.las[t] = las[t];
-    laser_band(c, las, K, &p.band_lo, &p.band_hi, &p.bandx_lo, &p.bandx_hi);
+    p.row0 = win ? win->row0 : 0;
+    p.gny = win ? win->gny : c.ny;
+    p.row_lo = win ? win->lo : 0;
+    p.row_hi = win ? win->hi : c.ny;
+    const int nrows = p.row_hi - p.row_lo;
+    if (win) {
+        // the source band in the field's rows, then in this buffer's
+        Coef g = c;
+        g.ny = p.gny;
+        laser_band(g, las, K, &p.band_lo, &p.band_hi, &p.bandx_lo, &p.bandx_hi);
+        p.band_lo = std::max(-2, std::min(p.band_lo - p.row0, c.ny + 2));
+        p.band_hi = std::max(-2, std::min(p.band_hi - p.row0, c.ny + 2));
+    } else {
+        laser_band(c, las, K, &p.band_lo, &p.band_hi, &p.bandx_lo, &p.bandx_hi);
+    }
     p.nstrips = (c.nx + ADV_WOUT - 1) / ADV_WOUT;
     // Dynamic scheduling (workspace given): short chunks, many tasks per
     // warp.  Static: about one task per resident warp.
@@ -161,12 +175,12 @@ cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const Laser
             H = 24;
         } else {
             const int want = std::max(1, (resident * ADV_WARPS) / p.nstrips);
-            H = (c.ny + want - 1) / want;
+            H = (nrows + want - 1) / want;
         }
         H = std::max(H, std::max(8, 4 * K));
     }
-    p.H = std::min(H, c.ny);
-    p.nchunks = (c.ny + p.H - 1) / p.H;
+    p.H = std::min(H, nrows);
+    p.nchunks = (nrows + p.H - 1) / p.H;
     p.ntasks = p.nstrips * p.nchunks;
     int grid = std::min((p.ntasks + ADV_WARPS - 1) / ADV_WARPS, resident);
     if (REDUCE && !ref_out) grid = std::min(grid, MAX_CTAS);
@@ -195,17 +209,17 @@ cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const Laser
 template <int K>
 cudaError_t launch_k(bool tma, bool reduce, const double* Tin, double* Tout, const Coef& c,
                      const LaserSub* las, Partial* ring, Workspace* ws, Partial* ref_out,
-                     long long ref_nparts, int rows, cudaStream_t s) {
+                     long long ref_nparts, int rows, cudaStream_t s, const RowWindow* w) {
     if (tma) {
         const cudaError_t e = reduce
-            ? launch_t<K, true, true>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s)
-            : launch_t<K, true, false>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s);
+            ? launch_t<K, true, true>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s, w)
+            : launch_t<K, true, false>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s, w);
         if (e != cudaErrorNotSupported) return e;
         // tensor map unavailable: fall through to the direct-load kernel
     }
     return reduce
-        ? launch_t<K, false, true>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s)
-        : launch_t<K, false, false>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s);
+        ? launch_t<K, false, true>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s, w)
+        : launch_t<K, false, false>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s, w);
 }
 
 }  // namespace
@@ -213,15 +227,15 @@ cudaError_t launch_k(bool tma, bool reduce, const double* Tin, double* Tout, con
 cudaError_t launch_advance(int K, const double* Tin, double* Tout, const Coef& c,
                            const LaserSub* las, Partial* ring, Workspace* ws,
                            Partial* ref_out, long long ref_nparts, int rows,
-                           cudaStream_t stream) {
+                           cudaStream_t stream, const RowWindow* win) {
     const bool tma = tma_ok(Tin, c.nx) && tma_ok(Tout, c.nx);
     const bool reduce = (ring != nullptr) || (ref_out != nullptr);
     if (reduce && !ref_out && !ws) return cudaErrorInvalidValue;
     switch (K) {
-        case 1: return launch_k<1>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream);
-        case 2: return launch_k<2>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream);
-        case 3: return launch_k<3>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream);
-        case 4: return launch_k<4>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream);
+        case 1: return launch_k<1>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream, win);
+        case 2: return launch_k<2>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream, win);
+        case 3: return launch_k<3>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream, win);
+        case 4: return launch_k<4>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream, win);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -327,6 +341,36 @@ int lpbf_b200_advance(double* T_a, double* T_b, const StepConst* k, const lpbf_t
     }
     *result_in_b = in_b;
     return LPBF_OK;
+}
+
+int lpbf_b200_advance_rows(const double* T_in, double* T_out, const StepConst* k,
+                           const lpbf_tick* plan, int n_steps, const lpbf_b200_opts* opts,
+                           const lpbf_b200_rows* rows, Partial* ring, void* work,
+                           size_t work_bytes, cudaStream_t stream) {
+    NvtxRange nvtx_range("lpbf_b200_advance_rows");
+    if (!valid_const(k) || !opts || !rows || !T_in || !T_out || n_steps < 1 || n_steps > 4 ||
+        !plan)
+        return LPBF_ERR_ARG;
+    if (opts->bc != 0 && opts->bc != 1) return LPBF_ERR_ARG;
+    if (opts->phys != 0) return LPBF_ERR_UNSUPPORTED;
+    const size_t N = (size_t)k->nx * k->ny;
+    if ((const double*)T_out < T_in + N && T_in < (const double*)T_out + N) return LPBF_ERR_ARG;
+    const RowWindow w{rows->row0, rows->global_ny, rows->lo, rows->hi};
+    if (w.row0 < 0 || w.gny < 1 || (long long)w.row0 + k->ny > w.gny ||
+        (long long)k->nx * w.gny >= (1ll << 40) || w.lo < 0 || w.lo >= w.hi || w.hi > k->ny)
+        return LPBF_ERR_ARG;
+    // the values of the advanced rows depend on n_steps rows either side
+    if (w.row0 > 0 && w.lo < n_steps) return LPBF_ERR_ARG;
+    if (w.row0 + k->ny < w.gny && k->ny - w.hi < n_steps) return LPBF_ERR_ARG;
+    Workspace* ws = static_cast<Workspace*>(work);
+    if (ring && (!ws || work_bytes < sizeof(Workspace))) return LPBF_ERR_WORKSPACE;
+    const Coef c = make_coef(*k, opts->bc, opts->T_edge, opts->Tm);
+    LaserSub las[KMAX];
+    for (int t = 0; t < n_steps; ++t)
+        las[t] = make_laser(*k, plan[t].x_l, plan[t].y_l, plan[t].q_scale);
+    const cudaError_t e = launch_advance(n_steps, T_in, T_out, c, las, ring, ws, nullptr, 0,
+                                         opts->rows, stream, &w);
+    return e == cudaSuccess ? LPBF_OK : LPBF_ERR_CUDA;
 }
 
 int lpbf_b200_read_error(const void* work, cudaStream_t stream, unsigned int* err) {

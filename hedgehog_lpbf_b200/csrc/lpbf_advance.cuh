@@ -77,6 +77,11 @@ struct AdvParams {
     Partial* ref_out;              // reference fused-reduce layout (K == 1), or null
     long long ref_nparts;          // number of entries of ref_out to define
     int st256;                     // 32-byte aligned rows: 256-bit stores
+    // Row window: the launch advances buffer rows [row_lo, row_hi) (the rest
+    // are input halo); buffer row 0 is row row0 of a field of gny rows, which
+    // places the source and numbers the cells in the reductions.  A whole
+    // field: row0 = 0, gny = ny, [0, ny).
+    int row0, gny, row_lo, row_hi;
 };
 
 __host__ __device__ constexpr int mod3(int a) { return ((a % 3) + 3) % 3; }
@@ -215,7 +220,7 @@ struct WarpStrip {
 
     // Neutral reduction state for every level (a new field for this warp).
     __device__ __forceinline__ void reset_red() {
-        const long long N = (long long)p.c.nx * p.c.ny;
+        const long long N = (long long)p.c.nx * p.gny;
         last_chunk = -1;
         if constexpr (REDUCE) {
 #pragma unroll
@@ -223,7 +228,7 @@ struct WarpStrip {
                 hit[t] = false;
                 rs->tmx[t][lane] = -1.0;
                 rs->arg[t][lane] = N;
-                if (lane == 0) { rs->ymn[t] = p.c.ny; rs->ymx[t] = -1; }
+                if (lane == 0) { rs->ymn[t] = p.gny; rs->ymx[t] = -1; }
             }
         }
         __syncwarp();
@@ -267,8 +272,8 @@ struct WarpStrip {
         x0 = strip * ADV_WOUT;
         xs = x0 - ADV_KH;
         xl = xs + 4 * lane;
-        y0 = chunk * p.H;
-        y1 = min(y0 + p.H, ny);
+        y0 = p.row_lo + chunk * p.H;
+        y1 = min(y0 + p.H, p.row_hi);
         jy0 = max(y0 - K, 0);
         jy0 -= jy0 % 3;
         jend = min(y1 + K, ny);
@@ -524,7 +529,7 @@ struct WarpStrip {
                 if (xl + v == nx - 1) R[v] = ce[v];
             }
         }
-        const double yd = __dsub_rn(__dmul_rn((double)r, c.dy), las.y_l);
+        const double yd = __dsub_rn(__dmul_rn((double)(r + p.row0), c.dy), las.y_l);
         const double dy2 = __dmul_rn(yd, yd);
         const bool src = las.cs != 0.0 && dy2 < c.r2_cut && src_strip;
         double4 S4 = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -640,13 +645,13 @@ struct WarpStrip {
                 // smallest flat index (NaN never wins)
                 const bool take = ok && val > m;
                 m = take ? val : m;
-                a = take ? (long long)r * nx + xl + v : a;
+                a = take ? (long long)(r + p.row0) * nx + xl + v : a;
                 hot |= ok && val > p.c.Tm;
                 nonfinite |= ok && !(fabs(val) < INFINITY);
             }
             if (__any_sync(0xffffffffu, hot) && lane == 0) {
-                rs->ymn[T - 1] = min(rs->ymn[T - 1], r);
-                rs->ymx[T - 1] = max(rs->ymx[T - 1], r);
+                rs->ymn[T - 1] = min(rs->ymn[T - 1], r + p.row0);
+                rs->ymx[T - 1] = max(rs->ymx[T - 1], r + p.row0);
             }
         }
         // a NaN or infinite temperature is reported, never trapped on; the
@@ -755,7 +760,7 @@ advance_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
         }
     }
 
-    const long long N = (long long)p.c.nx * p.c.ny;
+    const long long N = (long long)p.c.nx * p.gny;
     if constexpr (REDUCE) {
 #pragma unroll
         __syncwarp();
@@ -769,7 +774,7 @@ advance_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
         __syncthreads();
         if (threadIdx.x < K) {
             const int t = threadIdx.x;
-            double tm = -1.0; long long ag = N; int mn = p.c.ny, mx = -1;
+            double tm = -1.0; long long ag = N; int mn = p.gny, mx = -1;
             for (int w = 0; w < ADV_WARPS; ++w)
                 partial_take(tm, ag, mn, mx, red[w][t].tmax, red[w][t].arg,
                              red[w][t].ymin, red[w][t].ymax);
@@ -779,7 +784,7 @@ advance_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
         if (p.ref_out) {
             // Reference layout: the caller finalizes ref_nparts entries, so
             // every entry past this grid's must hold the neutral element.
-            const Partial neutral{-1.0, N, p.c.ny, -1};
+            const Partial neutral{-1.0, N, p.gny, -1};
             for (long long i = gridDim.x + (long long)blockIdx.x * blockDim.x + threadIdx.x;
                  i < p.ref_nparts; i += (long long)gridDim.x * blockDim.x)
                 p.ref_out[i] = neutral;
@@ -797,7 +802,7 @@ advance_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
     if constexpr (REDUCE) {
         if (p.ring) {
             for (int t = 0; t < K; ++t) {
-                double tm = -1.0; long long ag = N; int mn = p.c.ny, mx = -1;
+                double tm = -1.0; long long ag = N; int mn = p.gny, mx = -1;
                 for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
                     const Partial* q = &p.scratch[(size_t)i * K + t];
                     partial_take(tm, ag, mn, mx, __ldcg(&q->tmax), __ldcg(&q->arg),
@@ -808,7 +813,7 @@ advance_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
                 if (lane == 0) red[wid][0] = Partial{tm, ag, mn, mx};
                 __syncthreads();
                 if (threadIdx.x == 0) {
-                    double a = -1.0; long long b = N; int c1 = p.c.ny, d1 = -1;
+                    double a = -1.0; long long b = N; int c1 = p.gny, d1 = -1;
                     for (int w = 0; w < ADV_WARPS; ++w)
                         partial_take(a, b, c1, d1, red[w][0].tmax, red[w][0].arg,
                                      red[w][0].ymin, red[w][0].ymax);

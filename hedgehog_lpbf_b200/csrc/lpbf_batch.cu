@@ -574,6 +574,10 @@ int lpbf_b200_batch_create(const lpbf_b200_scenario* sc, int n_scen, int n_steps
         p.H = lay.H[i];
         p.nchunks = (k.ny + p.H - 1) / p.H;
         p.ntasks = p.nstrips * p.nchunks;
+        p.row0 = 0;
+        p.gny = k.ny;
+        p.row_lo = 0;
+        p.row_hi = k.ny;
         p.st256 = (k.nx % 4 == 0) && reinterpret_cast<uintptr_t>(s.T_a) % 32 == 0 &&
                   reinterpret_cast<uintptr_t>(s.T_b) % 32 == 0;
         b.buf[0] = s.T_a;

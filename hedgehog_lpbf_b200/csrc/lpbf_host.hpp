@@ -85,11 +85,14 @@ inline bool tma_ok(const void* p, int nx) {
 // Baseline-physics advance of `K` steps in one launch (K = 1..4).
 //   ring   : K finalized Partials (null: no reduction)
 //   ref_out: reference fused-reduce layout (K == 1 only), ref_nparts entries
+//   win    : row window of a row-strip shard (null: the whole field; c.ny is
+//            then the buffer's rows and win->gny the field's)
 // Returns a CUDA error code.
+struct RowWindow { int row0, gny, lo, hi; };
 cudaError_t launch_advance(int K, const double* Tin, double* Tout, const Coef& c,
                            const LaserSub* las, Partial* ring, Workspace* ws,
                            Partial* ref_out, long long ref_nparts, int rows,
-                           cudaStream_t stream);
+                           cudaStream_t stream, const RowWindow* win = nullptr);
 
 // Extended-physics (phys == 1) single step, one thread per cell, with the
 // same reduction outputs as launch_advance.

@@ -91,6 +91,34 @@ int lpbf_b200_advance(double* T_a, double* T_b, const StepConst* k,
 /* Number of launches lpbf_b200_advance issues for these arguments. */
 int lpbf_b200_advance_launches(int nx, int ny, int n_steps, const lpbf_b200_opts* opts);
 
+/* A row strip of a larger field: the buffers hold rows row0 .. row0+k->ny-1
+ * of a field of global_ny rows (k->ny is the buffer's row count, every other
+ * StepConst member is the field's), and the call advances buffer rows
+ * [lo, hi); the rows outside are halo, read but not written. */
+typedef struct lpbf_b200_rows {
+    int row0;        /* field row of buffer row 0 */
+    int global_ny;   /* rows of the whole field */
+    int lo, hi;      /* buffer rows advanced */
+} lpbf_b200_rows;
+
+/* One launch of n_steps (1..4) baseline steps over a row strip, T_in ->
+ * T_out (rows [lo, hi) of T_out written, nothing else).  The results of
+ * rows [lo, hi) equal those of lpbf_b200_advance on the whole field bit for
+ * bit, provided the halo rows hold the field's values: at least n_steps halo
+ * rows above lo unless row0 == 0 (buffer row 0 is the field's top edge),
+ * at least n_steps below hi unless row0 + k->ny == global_ny (the bottom
+ * edge); otherwise LPBF_ERR_ARG.  ring (device, nullable) receives one
+ * Partial per step over rows [lo, hi) in the field's numbering (flat index
+ * (row0 + r) * nx + x, molten rows as field rows, neutral elements from
+ * global_ny); the Partials of all strips combine by the reduction's rule
+ * into the whole field's.  Row-strip sharding across GPUs: each rank
+ * advances its strip, then exchanges n_steps halo rows with its neighbours.
+ * No counterpart in the reference, which advances whole fields only. */
+int lpbf_b200_advance_rows(const double* T_in, double* T_out, const StepConst* k,
+                           const lpbf_tick* plan, int n_steps, const lpbf_b200_opts* opts,
+                           const lpbf_b200_rows* rows, Partial* ring, void* work,
+                           size_t work_bytes, cudaStream_t stream);
+
 /* Copy the workspace error word to *err (synchronizes `stream`); bit 0 means
  * a TMA wait exceeded its time limit and the launch stopped early; bit 1
  * means a computed temperature was NaN or infinite (baseline FP64 advance
