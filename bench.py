@@ -365,6 +365,55 @@ def superstep_leg(args, dev):
     return out
 
 
+def sharded_leg(args, dev, rank=0, world=1, single_value=None):
+    """One 8192^2 field cut into row strips: across the ranks (one strip
+    each, halo rows exchanged over NCCL after every launch; strong scaling),
+    or, on one GPU, into 4 strips exchanged by device copies (the cost of
+    the cut and of the exchange).  On one GPU the result is checked bit for
+    bit against the single-field solver."""
+    import torch
+    from hedgehog_lpbf_b200.sharded import ShardedField
+    from hedgehog_lpbf_b200.solver import Solver
+    mat, pr, dom, k, plan = workload(0)
+    depth = 3
+    n_warm, n = 30, args.sh_steps
+    kw = dict(depth=depth, device=dev, T0=300.0, Tm=mat.Tm)
+    if world > 1:
+        f = ShardedField.distributed(k, rank, world, **kw)
+        parts, kind = world, "NCCL send/recv between ranks"
+    else:
+        f = ShardedField.local(k, 4, **kw)
+        parts, kind = 4, "device copies within one GPU"
+    f.advance(plan[:n_warm], rings=False)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    rings = f.advance(plan[n_warm:n_warm + n])
+    e1.record()
+    torch.cuda.synchronize()
+    from hedgehog_lpbf_b200.ranks import max_over_ranks
+    ms = max_over_ranks(e0.elapsed_time(e1), dev)
+    out = {"value": dom.nx * dom.ny * n / (ms * 1e-3) / 1e9, "unit": "GCell-updates/s",
+           "strips": parts, "halo_rows": depth, "exchange": kind, "time_steps": n, "ms": ms,
+           "scaling": "strong (one field)" if world > 1 else "one GPU",
+           "error_word": f.stepper.read_error()}
+    parts_ring = f.partials(rings)
+    if world == 1:
+        s = Solver(k, device=dev, Tm=mat.Tm, depth=depth, T0=300.0)
+        s.advance(plan[:n_warm])
+        r = s.new_ring(n)
+        s.advance(plan[n_warm:n_warm + n], r)
+        same = torch.equal(f.field(), s.field)
+        out["bit_identical_to_single_field"] = bool(
+            same and parts_ring.tobytes() == r.cpu().numpy().tobytes())
+        if single_value:
+            out["vs_single_field"] = out["value"] / single_value
+        del s
+    return out
+
+
 def run_b200_arm(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -462,9 +511,10 @@ def run_b200_arm(args, rank, world, local_rank):
                 "bytes_per_update": 16}
         del sk, T64
 
+    del s
+    sh = sharded_leg(args, dev, rank, world, value / world) if args.sharded else None
     pm = None
     if args.process_map:
-        del s
         pm = process_map_leg(args, dev, rank, world)
     ss = None
     if args.superstep and world == 1:
@@ -498,6 +548,7 @@ def run_b200_arm(args, rank, world, local_rank):
         "gpu_launches": launches * args.steps,
         "f32k": f32k,
         "process_map": pm,
+        "sharded": sh,
         "superstep": ss,
         "clocks": clk.summary(),
         "error_word": err,
@@ -522,6 +573,9 @@ def main():
                     help="skip the FP32 compensated leg")
     ap.add_argument("--no-process-map", dest="process_map", action="store_false",
                     help="skip the batched process-map leg")
+    ap.add_argument("--no-sharded", dest="sharded", action="store_false",
+                    help="skip the row-strip sharded leg")
+    ap.add_argument("--sh-steps", type=int, default=300)
     ap.add_argument("--pm-scenarios", type=int, default=256)
     ap.add_argument("--pm-steps", type=int, default=5000)
     ap.add_argument("--no-superstep", dest="superstep", action="store_false",
