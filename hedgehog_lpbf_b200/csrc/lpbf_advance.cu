@@ -166,13 +166,17 @@ cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const Laser
         laser_band(c, las, K, &p.band_lo, &p.band_hi, &p.bandx_lo, &p.bandx_hi);
     }
     p.nstrips = (c.nx + ADV_WOUT - 1) / ADV_WOUT;
-    // Dynamic scheduling (workspace given): short chunks, many tasks per
-    // warp.  Static: about one task per resident warp.
+    // Dynamic scheduling (workspace given): several tasks per warp from the
+    // atomic queue.  Static: about one task per resident warp.
     const bool dynamic = ws != nullptr;
     int H = rows;
     if (H <= 0) {
         if (dynamic) {
-            H = 24;
+            // about three tasks per resident warp, 12..64 rows: tall tasks
+            // cost less halo, and the band split keeps the slow source-band
+            // tasks short whatever H is
+            const long long want = (long long)nrows * p.nstrips / (3ll * resident * ADV_WARPS);
+            H = (int)std::max(12ll, std::min(64ll, want));
         } else {
             const int want = std::max(1, (resident * ADV_WARPS) / p.nstrips);
             H = (nrows + want - 1) / want;
@@ -180,7 +184,21 @@ cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const Laser
         H = std::max(H, std::max(8, 4 * K));
     }
     p.H = std::min(H, nrows);
-    p.nchunks = (nrows + p.H - 1) / p.H;
+    p.Ya = p.Yb = p.row_lo;
+    p.Hb = p.H;
+    if (dynamic && p.band_lo <= p.band_hi) {
+        // rows whose tasks (owned rows +- K) reach the source band
+        const int b0 = std::max(p.row_lo, p.band_lo - K);
+        const int b1 = std::min(p.row_hi, p.band_hi + K + 1);
+        if (b0 < b1) {
+            p.Hb = std::min(p.H, ADV_BAND_ROWS);
+            p.nA = (b0 - p.row_lo) / p.H;
+            p.Ya = p.row_lo + p.nA * p.H;
+            p.Yb = b1;
+            p.nB = (p.Yb - p.Ya + p.Hb - 1) / p.Hb;
+        }
+    }
+    p.nchunks = p.nA + p.nB + (p.row_hi - p.Yb + p.H - 1) / p.H;
     p.ntasks = p.nstrips * p.nchunks;
     int grid = std::min((p.ntasks + ADV_WARPS - 1) / ADV_WARPS, resident);
     if (REDUCE && !ref_out) grid = std::min(grid, MAX_CTAS);

@@ -56,6 +56,7 @@ constexpr int ADV_WOUT = ADV_COLS - 2 * ADV_KH;
 constexpr int ADV_V = 4;           // values per lane per row
 constexpr int ADV_R = 3;           // rows per TMA box (= the register slot rotation)
 constexpr int ADV_S = 4;           // TMA stages per warp
+constexpr int ADV_BAND_ROWS = 8;   // rows per task where tasks reach the source band
 constexpr int ADV_STAGE_DOUBLES = ADV_R * ADV_COLS;
 constexpr size_t ADV_SMEM_BYTES =
     size_t(ADV_WARPS) * ADV_S * ADV_STAGE_DOUBLES * sizeof(double)
@@ -82,6 +83,11 @@ struct AdvParams {
     // places the source and numbers the cells in the reductions.  A whole
     // field: row0 = 0, gny = ny, [0, ny).
     int row0, gny, row_lo, row_hi;
+    // Chunks: nA of H rows from row_lo, then nB of Hb rows from Ya up to Yb
+    // (the rows whose tasks reach the source band: short tasks, so that
+    // none of these slow ones is left long at the end of a launch), then
+    // H-row chunks from Yb.  No band split: nA = nB = 0, Ya = Yb = row_lo.
+    int nA, nB, Hb, Ya, Yb;
 };
 
 __host__ __device__ constexpr int mod3(int a) { return ((a % 3) + 3) % 3; }
@@ -272,8 +278,16 @@ struct WarpStrip {
         x0 = strip * ADV_WOUT;
         xs = x0 - ADV_KH;
         xl = xs + 4 * lane;
-        y0 = p.row_lo + chunk * p.H;
-        y1 = min(y0 + p.H, p.row_hi);
+        if (chunk < p.nA) {
+            y0 = p.row_lo + chunk * p.H;
+            y1 = y0 + p.H;
+        } else if (chunk < p.nA + p.nB) {
+            y0 = p.Ya + (chunk - p.nA) * p.Hb;
+            y1 = min(y0 + p.Hb, p.Yb);
+        } else {
+            y0 = p.Yb + (chunk - p.nA - p.nB) * p.H;
+            y1 = min(y0 + p.H, p.row_hi);
+        }
         jy0 = max(y0 - K, 0);
         jy0 -= jy0 % 3;
         jend = min(y1 + K, ny);
