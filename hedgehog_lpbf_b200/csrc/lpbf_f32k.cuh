@@ -43,6 +43,7 @@ struct FkParams {
     LaserSub las[KMAX];
     int band_lo, band_hi, bandx_lo, bandx_hi;
     int nstrips, nchunks, H, ntasks;
+    int nA, nB, Hb, Ya, Yb;        // band-split chunks, as in AdvParams
     float* Thi_out;
     float* Tlo_out;
     Partial* ring;
@@ -150,8 +151,16 @@ struct FkStrip {
         x0 = strip * ADV_WOUT;
         xs = x0 - ADV_KH;
         xl = xs + 4 * lane;
-        y0 = chunk * p.H;
-        y1 = min(y0 + p.H, ny);
+        if (chunk < p.nA) {
+            y0 = chunk * p.H;
+            y1 = y0 + p.H;
+        } else if (chunk < p.nA + p.nB) {
+            y0 = p.Ya + (chunk - p.nA) * p.Hb;
+            y1 = min(y0 + p.Hb, p.Yb);
+        } else {
+            y0 = p.Yb + (chunk - p.nA - p.nB) * p.H;
+            y1 = min(y0 + p.H, ny);
+        }
         jy0 = max(y0 - K, 0);
         jy0 -= jy0 % 3;
         jend = min(y1 + K, ny);
