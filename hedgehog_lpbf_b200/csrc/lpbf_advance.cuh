@@ -92,23 +92,29 @@ struct AdvParams {
 
 __host__ __device__ constexpr int mod3(int a) { return ((a % 3) + 3) % 3; }
 
-// Hot coefficients, held in registers for the whole kernel.
+// Hot coefficients, held in registers for the whole kernel (clsTa is
+// c_ls * Tamb, rounded once).
 struct HotCoef {
-    double ax, ay, cls, crad, Ta, Ta4;
+    double ax, ay, cls, crad, clsTa, Ta4;
 };
+__device__ __forceinline__ HotCoef hot_coef(const Coef& c) {
+    return HotCoef{c.ax, c.ay, c.c_ls, c.c_rad, __dmul_rn(c.c_ls, c.Tamb), c.Tamb4};
+}
 
-// The update of one cell from its four neighbours (Tamb == Tsub form).  The
-// multiplies and fused multiply-adds are spelled out so that the compiler
-// cannot contract differently in different call sites: every path computes a
-// cell bit-identically.  Every term vanishes exactly for a uniform field at
-// Tamb.
+// The update of one cell from its four neighbours (Tamb == Tsub form), in
+// 12 FP64 operations: T^4 - Tamb^4 and c_ls (T - Tamb) are each one fused
+// multiply-add.  The operations are spelled out so that the compiler cannot
+// contract differently in different call sites: every path computes a cell
+// bit-identically.  For a uniform field at Tamb both loss terms leave only
+// their last rounding (|loss| ~ 1e-16 K), below half an ulp of T, so such a
+// field stays exactly uniform.
 __device__ __forceinline__ double cell_inc(double T, double L, double R, double U, double D,
                                            const HotCoef& h, double& loss) {
     const double lx = fma(-2.0, T, R + L);
     const double ly = fma(-2.0, T, U + D);
     const double t2 = __dmul_rn(T, T);
-    const double e4 = __dsub_rn(__dmul_rn(t2, t2), h.Ta4);
-    loss = fma(h.crad, e4, __dmul_rn(h.cls, __dsub_rn(T, h.Ta)));
+    const double e4 = fma(t2, t2, -h.Ta4);
+    loss = fma(h.crad, e4, fma(h.cls, T, -h.clsTa));
     return fma(h.ax, lx, __dmul_rn(h.ay, ly));
 }
 __device__ __forceinline__ double cell_core(double T, double L, double R, double U, double D,
@@ -213,7 +219,7 @@ struct WarpStrip {
                                          double* st, uint64_t* b, int ln, RedSmem<K>* rs_,
                                          uint32_t gbox0 = 0)
         : p(p_), map(m), stages(st), bars(b), gbox(gbox0), lane(ln),
-          h{p_.c.ax, p_.c.ay, p_.c.c_ls, p_.c.c_rad, p_.c.Tamb, p_.c.Tamb4},
+          h(hot_coef(p_.c)),
           last_chunk(-1), failed(false), incl(false), kmask(0u), rs(rs_) {
         reset_red();
     }
@@ -221,7 +227,7 @@ struct WarpStrip {
     // Re-read the hot coefficients after the parameters behind `p` changed
     // (the batched kernel rebinds one WarpStrip to another field per task).
     __device__ __forceinline__ void reload_coef() {
-        h = HotCoef{p.c.ax, p.c.ay, p.c.c_ls, p.c.c_rad, p.c.Tamb, p.c.Tamb4};
+        h = hot_coef(p.c);
     }
 
     // Neutral reduction state for every level (a new field for this warp).

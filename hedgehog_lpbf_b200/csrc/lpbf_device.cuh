@@ -12,10 +12,11 @@
 //     T' = T + dt * ( alpha*(lap_x + lap_y) + S - loss(T) )
 // with every dt-scaled coefficient folded on the host:
 //     T' = T + ( ax*(R + L - 2T) + ay*(U + D - 2T) + S_dt - loss_dt(T) ).
-// Each term is kept as a difference that is exactly zero at equilibrium
-// (uniform field at the ambient temperature), so untouched far-field cells
-// stay bit-exactly at T_amb, as in the reference; all other differences are
-// rounding of the increment, far below 1e-12 of T.
+// At equilibrium (uniform field at the ambient temperature) every term is
+// zero or, in the fused Tamb == Tsub form of the step kernel, a last rounding
+// far below half an ulp of T, so untouched far-field cells stay bit-exactly
+// at T_amb, as in the reference; all other differences are rounding of the
+// increment, far below 1e-12 of T.
 // ---------------------------------------------------------------------------
 #pragma once
 #include <cuda.h>
