@@ -102,32 +102,29 @@ __device__ __forceinline__ HotCoef hot_coef(const Coef& c) {
 }
 
 // The update of one cell from its four neighbours (Tamb == Tsub form), in
-// 12 FP64 operations: T^4 - Tamb^4 and c_ls (T - Tamb) are each one fused
-// multiply-add.  The operations are spelled out so that the compiler cannot
-// contract differently in different call sites: every path computes a cell
-// bit-identically.  For a uniform field at Tamb both loss terms leave only
-// their last rounding (|loss| ~ 1e-16 K), below half an ulp of T, so such a
-// field stays exactly uniform.
-__device__ __forceinline__ double cell_inc(double T, double L, double R, double U, double D,
-                                           const HotCoef& h, double& loss) {
+// 11 FP64 operations: T^4 - Tamb^4 and c_ls (T - Tamb) are each one fused
+// multiply-add, and the loss enters the increment's fused chain.  The
+// operations are spelled out so that the compiler cannot contract
+// differently in different call sites: every path computes a cell
+// bit-identically.  For a uniform field at Tamb the loss is only a last
+// rounding (|loss| ~ 1e-16 K), below half an ulp of T, so such a field stays
+// exactly uniform.
+__device__ __forceinline__ double cell_net(double T, double L, double R, double U, double D,
+                                           const HotCoef& h) {
     const double lx = fma(-2.0, T, R + L);
     const double ly = fma(-2.0, T, U + D);
     const double t2 = __dmul_rn(T, T);
     const double e4 = fma(t2, t2, -h.Ta4);
-    loss = fma(h.crad, e4, fma(h.cls, T, -h.clsTa));
-    return fma(h.ax, lx, __dmul_rn(h.ay, ly));
+    const double loss = fma(h.crad, e4, fma(h.cls, T, -h.clsTa));
+    return fma(h.ax, lx, fma(h.ay, ly, -loss));
 }
 __device__ __forceinline__ double cell_core(double T, double L, double R, double U, double D,
                                             const HotCoef& h) {
-    double loss;
-    const double inc = cell_inc(T, L, R, U, D, h, loss);
-    return __dadd_rn(T, __dsub_rn(inc, loss));
+    return __dadd_rn(T, cell_net(T, L, R, U, D, h));
 }
 __device__ __forceinline__ double cell_core_src(double T, double L, double R, double U, double D,
                                                 double S, const HotCoef& h) {
-    double loss;
-    const double inc = cell_inc(T, L, R, U, D, h, loss);
-    return __dadd_rn(T, __dsub_rn(__dadd_rn(inc, S), loss));
+    return __dadd_rn(T, __dadd_rn(cell_net(T, L, R, U, D, h), S));
 }
 
 // Gaussian source increment of a lane's four cells starting at column x0
