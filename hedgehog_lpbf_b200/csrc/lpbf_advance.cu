@@ -121,11 +121,11 @@ bool tensor_map_act_bf16(const void* base, int C, int W, int H, int B, int box_p
 // ---- launch of one temporally blocked step ---------------------------------
 namespace {
 
-template <int K, bool TMA, bool REDUCE>
+template <int K, bool TMA, bool REDUCE, bool SQ>
 cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const LaserSub* las,
                      Partial* ring, Workspace* ws, Partial* ref_out, long long ref_nparts,
                      int rows, cudaStream_t stream, const RowWindow* win) {
-    auto kern = advance_kernel<K, TMA, REDUCE>;
+    auto kern = advance_kernel<K, TMA, REDUCE, SQ>;
     const size_t smem = TMA ? ADV_SMEM_BYTES : 0;
 
     static int occ[64] = {0};
@@ -224,20 +224,36 @@ cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const Laser
     return cudaGetLastError();
 }
 
-template <int K>
-cudaError_t launch_k(bool tma, bool reduce, const double* Tin, double* Tout, const Coef& c,
-                     const LaserSub* las, Partial* ring, Workspace* ws, Partial* ref_out,
-                     long long ref_nparts, int rows, cudaStream_t s, const RowWindow* w) {
+template <int K, bool SQ>
+cudaError_t launch_k2(bool tma, bool reduce, const double* Tin, double* Tout, const Coef& c,
+                      const LaserSub* las, Partial* ring, Workspace* ws, Partial* ref_out,
+                      long long ref_nparts, int rows, cudaStream_t s, const RowWindow* w) {
     if (tma) {
         const cudaError_t e = reduce
-            ? launch_t<K, true, true>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s, w)
-            : launch_t<K, true, false>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s, w);
+            ? launch_t<K, true, true, SQ>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows,
+                                          s, w)
+            : launch_t<K, true, false, SQ>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows,
+                                           s, w);
         if (e != cudaErrorNotSupported) return e;
         // tensor map unavailable: fall through to the direct-load kernel
     }
     return reduce
-        ? launch_t<K, false, true>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s, w)
-        : launch_t<K, false, false>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s, w);
+        ? launch_t<K, false, true, SQ>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s, w)
+        : launch_t<K, false, false, SQ>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s,
+                                        w);
+}
+
+// Square cells (ax == ay, the same comparison the kernels make) take the
+// one-Laplacian form of the cell update.
+template <int K>
+cudaError_t launch_k(bool tma, bool reduce, const double* Tin, double* Tout, const Coef& c,
+                     const LaserSub* las, Partial* ring, Workspace* ws, Partial* ref_out,
+                     long long ref_nparts, int rows, cudaStream_t s, const RowWindow* w) {
+    return c.ax == c.ay
+        ? launch_k2<K, true>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows,
+                             s, w)
+        : launch_k2<K, false>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows,
+                              s, w);
 }
 
 }  // namespace

@@ -93,38 +93,48 @@ struct AdvParams {
 __host__ __device__ constexpr int mod3(int a) { return ((a % 3) + 3) % 3; }
 
 // Hot coefficients, held in registers for the whole kernel (clsTa is
-// c_ls * Tamb, rounded once).
+// c_ls * Tamb, rounded once; sq: ax == ay, square cells).
 struct HotCoef {
     double ax, ay, cls, crad, clsTa, Ta4;
+    bool sq;
 };
 __device__ __forceinline__ HotCoef hot_coef(const Coef& c) {
-    return HotCoef{c.ax, c.ay, c.c_ls, c.c_rad, __dmul_rn(c.c_ls, c.Tamb), c.Tamb4};
+    return HotCoef{c.ax, c.ay, c.c_ls, c.c_rad, __dmul_rn(c.c_ls, c.Tamb), c.Tamb4,
+                   c.ax == c.ay};
 }
 
-// The update of one cell from its four neighbours (Tamb == Tsub form), in
-// 11 FP64 operations: T^4 - Tamb^4 and c_ls (T - Tamb) are each one fused
-// multiply-add, and the loss enters the increment's fused chain.  The
-// operations are spelled out so that the compiler cannot contract
-// differently in different call sites: every path computes a cell
-// bit-identically.  For a uniform field at Tamb the loss is only a last
-// rounding (|loss| ~ 1e-16 K), below half an ulp of T, so such a field stays
-// exactly uniform.
+// The update of one cell from its four neighbours (Tamb == Tsub form).
+// T^4 - Tamb^4 and c_ls (T - Tamb) are each one fused multiply-add and the
+// loss enters the increment's fused chain: 11 FP64 operations, or 10 when
+// ax == ay (SQ: one Laplacian (R + L) + (U + D) - 4T).  Which form a field
+// uses depends only on its coefficients, so every path computes a cell
+// bit-identically.  The Laplacian is exactly zero for a uniform field, and
+// the loss at Tamb is only a last rounding (|loss| ~ 1e-16 K), below half an
+// ulp of T, so a uniform field at Tamb stays exactly uniform.
+template <bool SQ>
 __device__ __forceinline__ double cell_net(double T, double L, double R, double U, double D,
                                            const HotCoef& h) {
-    const double lx = fma(-2.0, T, R + L);
-    const double ly = fma(-2.0, T, U + D);
     const double t2 = __dmul_rn(T, T);
     const double e4 = fma(t2, t2, -h.Ta4);
     const double loss = fma(h.crad, e4, fma(h.cls, T, -h.clsTa));
-    return fma(h.ax, lx, fma(h.ay, ly, -loss));
+    if constexpr (SQ) {
+        const double lap = fma(-4.0, T, __dadd_rn(R + L, U + D));
+        return fma(h.ax, lap, -loss);
+    } else {
+        const double lx = fma(-2.0, T, R + L);
+        const double ly = fma(-2.0, T, U + D);
+        return fma(h.ax, lx, fma(h.ay, ly, -loss));
+    }
 }
+template <bool SQ>
 __device__ __forceinline__ double cell_core(double T, double L, double R, double U, double D,
                                             const HotCoef& h) {
-    return __dadd_rn(T, cell_net(T, L, R, U, D, h));
+    return __dadd_rn(T, cell_net<SQ>(T, L, R, U, D, h));
 }
+template <bool SQ>
 __device__ __forceinline__ double cell_core_src(double T, double L, double R, double U, double D,
                                                 double S, const HotCoef& h) {
-    return __dadd_rn(T, __dadd_rn(cell_net(T, L, R, U, D, h), S));
+    return __dadd_rn(T, __dadd_rn(cell_net<SQ>(T, L, R, U, D, h), S));
 }
 
 // Gaussian source increment of a lane's four cells starting at column x0
@@ -175,7 +185,10 @@ static_assert(offsetof(RedSmem<3>, box) % 16 == 0 && sizeof(RedSmem<3>) % 16 == 
 // copy, which matters when warps work on many different fields at once (a
 // tensor map in global memory is fetched by the copy engine); requires an
 // even row length and a 16-byte aligned field.
-template <int K, bool TMA, bool REDUCE, bool BULK = false>
+// SQM: which cell_net form the strip uses — 0 the general one, 1 the
+// square-cell one, 2 the field's own (h.sq), chosen per task (the batched
+// kernel, whose fields differ).
+template <int K, bool TMA, bool REDUCE, bool BULK = false, int SQM = 0>
 struct WarpStrip {
     static constexpr int V = ADV_V;
 
@@ -324,9 +337,12 @@ struct WarpStrip {
             const bool fast = fast_ok && j - K >= 1 && j + 1 <= ny - 2 &&
                               (!src_strip || j + 1 < p.band_lo || j - K > p.band_hi);
             if (fast && j < jend) {
-                fast_row<0>(j, st);
-                fast_row<1>(j + 1, st);
-                fast_row<2>(j + 2, st);
+                if constexpr (SQM == 2) {
+                    if (h.sq) fast_box<true>(j, st);
+                    else      fast_box<false>(j, st);
+                } else {
+                    fast_box<SQM == 1>(j, st);
+                }
             } else {
                 general_row<0>(j, st, jlast);
                 general_row<1>(j + 1, st, jlast);
@@ -422,14 +438,21 @@ struct WarpStrip {
         }
     }
 
-    template <int P>
+    template <bool SQ>
+    __device__ __forceinline__ void fast_box(int j, const double* st) {
+        fast_row<0, SQ>(j, st);
+        fast_row<1, SQ>(j + 1, st);
+        fast_row<2, SQ>(j + 2, st);
+    }
+
+    template <int P, bool SQ>
     __device__ __forceinline__ void fast_row(int jj, const double* st) {
         load_row0<P>(jj, st, win<0>()[P]);
         if (mir) mirror_fix(win<0>()[P]);
-        fast_level<P, 1>(jj);
+        fast_level<P, 1, SQ>(jj);
     }
 
-    template <int P, int T>
+    template <int P, int T, bool SQ>
     __device__ __forceinline__ void fast_level(int jj) {
         if constexpr (T <= K) {
             constexpr int su = mod3(P - T - 1), sc = mod3(P - T), sd = mod3(P - T + 1);
@@ -440,10 +463,10 @@ struct WarpStrip {
             double Lo, Ro;
             neighbours(ce, Lo, Ro);
             double nv[V];
-            nv[0] = cell_core(ce[0], Lo, ce[1], up[0], dn[0], h);
-            nv[1] = cell_core(ce[1], ce[0], ce[2], up[1], dn[1], h);
-            nv[2] = cell_core(ce[2], ce[1], ce[3], up[2], dn[2], h);
-            nv[3] = cell_core(ce[3], ce[2], Ro, up[3], dn[3], h);
+            nv[0] = cell_core<SQ>(ce[0], Lo, ce[1], up[0], dn[0], h);
+            nv[1] = cell_core<SQ>(ce[1], ce[0], ce[2], up[1], dn[1], h);
+            nv[2] = cell_core<SQ>(ce[2], ce[1], ce[3], up[2], dn[2], h);
+            nv[3] = cell_core<SQ>(ce[3], ce[2], Ro, up[3], dn[3], h);
             const int r = jj - T;
             // Rows outside [y0, y1) are this chunk's halo: computed (their
             // values only ever feed other halo rows) but not stored or reduced.
@@ -462,7 +485,7 @@ struct WarpStrip {
             if constexpr (REDUCE) {
                 if (owned_row) row_stats<T - 1, P>(r, nv, own_all, true);
             }
-            fast_level<P, T + 1>(jj);
+            fast_level<P, T + 1, SQ>(jj);
         }
     }
 
@@ -521,6 +544,19 @@ struct WarpStrip {
         }
     }
 
+    // The general body's cell update in this strip's form.
+    __device__ __forceinline__ double gcore(double T, double L, double R, double U, double D) {
+        if constexpr (SQM == 2) return h.sq ? cell_core<true>(T, L, R, U, D, h)
+                                            : cell_core<false>(T, L, R, U, D, h);
+        else return cell_core<SQM == 1>(T, L, R, U, D, h);
+    }
+    __device__ __forceinline__ double gcore_src(double T, double L, double R, double U, double D,
+                                                double S) {
+        if constexpr (SQM == 2) return h.sq ? cell_core_src<true>(T, L, R, U, D, S, h)
+                                            : cell_core_src<false>(T, L, R, U, D, S, h);
+        else return cell_core_src<SQM == 1>(T, L, R, U, D, S, h);
+    }
+
     __device__ __forceinline__ bool owned_lane() const {
         return xl >= x0 && xl < x0 + ADV_WOUT && xl < p.c.nx;
     }
@@ -555,8 +591,8 @@ struct WarpStrip {
         if (c.same_T) {
 #pragma unroll
             for (int v = 0; v < V; ++v)
-                nv[v] = src ? cell_core_src(ce[v], L[v], R[v], up[v], dn[v], S[v], h)
-                            : cell_core(ce[v], L[v], R[v], up[v], dn[v], h);
+                nv[v] = src ? gcore_src(ce[v], L[v], R[v], up[v], dn[v], S[v])
+                            : gcore(ce[v], L[v], R[v], up[v], dn[v]);
         } else {
 #pragma unroll
             for (int v = 0; v < V; ++v)
@@ -736,7 +772,7 @@ struct WarpStrip {
 template <int K>
 struct AdvOcc { static constexpr int min_ctas = 3; };
 
-template <int K, bool TMA, bool REDUCE>
+template <int K, bool TMA, bool REDUCE, bool SQ>
 __global__ void __launch_bounds__(ADV_WARPS * 32, AdvOcc<K>::min_ctas)
 advance_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ AdvParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -758,7 +794,8 @@ advance_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
         __syncwarp();
     }
 
-    WarpStrip<K, TMA, REDUCE> ws(p, &map, stages, bars, lane, &s_red[REDUCE ? wid : 0]);
+    WarpStrip<K, TMA, REDUCE, false, SQ ? 1 : 0> ws(p, &map, stages, bars, lane,
+                                                    &s_red[REDUCE ? wid : 0]);
     if (p.tasks) {
         // dynamic: lane 0 draws the next task for the warp
         for (;;) {

@@ -113,7 +113,9 @@ __device__ __forceinline__ void fold(const BatchLaunch& L, int s, int i, int bas
 struct TaskCtx { int tq, s, base, nt; };
 
 // ST: 0 direct loads, 1 bulk row copies, 2 tensor-map tiles (BATCH_STAGE_*).
-template <int K, int ST>
+// SQM: 1 every field has square cells (one form of the cell update), 2 each
+// field takes its own form per task (the WarpStrip modes).
+template <int K, int ST, int SQM>
 __global__ void __launch_bounds__(ADV_WARPS * 32, AdvOcc<K>::min_ctas)
 batch_kernel(const __grid_constant__ BatchLaunch L) {
     constexpr bool STAGED = ST != BATCH_STAGE_DIRECT;
@@ -142,7 +144,7 @@ batch_kernel(const __grid_constant__ BatchLaunch L) {
         for (int i = lane; i < (int)(sizeof(AdvParams) / 8); i += 32) d[i] = 0ull;
         __syncwarp();
     }
-    WarpStrip<K, STAGED, true, ST == BATCH_STAGE_BULK> ws(par, nullptr, stages, bars, lane,
+    WarpStrip<K, STAGED, true, ST == BATCH_STAGE_BULK, SQM> ws(par, nullptr, stages, bars, lane,
                                                          &s_red[wid]);
     volatile TaskCtx* ctx = &s_ctx[wid];
     int bound = -1;                // scenario whose parameters sit in `par`
@@ -241,16 +243,19 @@ struct BatchKernelInfo {
         cudaGetDevice(&dev);
         if (dev < 0 || dev >= 64) dev = 0;
         if (occ[dev] == 0) {
-            auto kern = batch_kernel<K, ST>;
             const size_t smem = STAGED ? ADV_SMEM_BYTES : 0;
-            if (smem > 48 * 1024 &&
-                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem) != cudaSuccess)
-                return 0;
-            int nb = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, ADV_WARPS * 32, smem) !=
-                cudaSuccess)
-                return 0;
+            int nb = 1 << 30;
+            for (auto kern : {batch_kernel<K, ST, 1>, batch_kernel<K, ST, 2>}) {
+                if (smem > 48 * 1024 &&
+                    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem) != cudaSuccess)
+                    return 0;
+                int n = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, ADV_WARPS * 32,
+                                                                  smem) != cudaSuccess)
+                    return 0;
+                nb = std::min(nb, n);
+            }
             occ[dev] = std::max(1, nb);
         }
         return occ[dev];
@@ -261,7 +266,9 @@ struct BatchKernelInfo {
         const int per_sm = ctas_per_sm > 0 ? std::min(ctas_per_sm, occ) : occ;
         int grid = std::min(sm_count() * per_sm, (L.ntasks + ADV_WARPS - 1) / ADV_WARPS);
         grid = std::max(grid, 1);
-        batch_kernel<K, ST><<<grid, ADV_WARPS * 32, STAGED ? ADV_SMEM_BYTES : 0, s>>>(L);
+        const size_t smem = STAGED ? ADV_SMEM_BYTES : 0;
+        if (L.sq_all) batch_kernel<K, ST, 1><<<grid, ADV_WARPS * 32, smem, s>>>(L);
+        else          batch_kernel<K, ST, 2><<<grid, ADV_WARPS * 32, smem, s>>>(L);
         return cudaGetLastError();
     }
 };
@@ -438,6 +445,7 @@ struct lpbf_b200_batch {
     unsigned char* work = nullptr;
     int cur = 0;                   // buffer holding the current fields (0: T_a, 1: T_b)
     bool all_rings = false;        // every scenario has a ring
+    bool sq_all = false;           // every scenario has square cells
     int device = 0;
     // cached graphs, keyed by (first_step, n_steps, starting parity)
     struct Graph { cudaGraphExec_t exec = nullptr; int first = -1, n = -1, par = -1; };
@@ -460,6 +468,7 @@ struct lpbf_b200_batch {
         L.ntasks = lay.ntasks;
         L.parity = parity;
         L.step0 = step0;
+        L.sq_all = sq_all ? 1 : 0;
         return L;
     }
 
@@ -563,6 +572,7 @@ int lpbf_b200_batch_create(const lpbf_b200_scenario* sc, int n_scen, int n_steps
     std::memset(img, 0, img_bytes);
     std::vector<BatchStep> steps((size_t)n_scen * n_steps);
     std::vector<BatchScen> scen(n_scen);
+    bool sq_all = true;
     for (int i = 0; i < n_scen; ++i) {
         const lpbf_b200_scenario& s = sc[lay.order[i]];
         const StepConst& k = *s.k;
@@ -570,6 +580,7 @@ int lpbf_b200_batch_create(const lpbf_b200_scenario* sc, int n_scen, int n_steps
         std::memset(&b, 0, sizeof(b));
         AdvParams& p = b.par;
         p.c = make_coef(k, s.bc, s.T_edge, s.Tm);
+        sq_all = sq_all && p.c.ax == p.c.ay;
         p.nstrips = (k.nx + ADV_WOUT - 1) / ADV_WOUT;
         p.H = lay.H[i];
         p.nchunks = (k.ny + p.H - 1) / p.H;
@@ -617,6 +628,7 @@ int lpbf_b200_batch_create(const lpbf_b200_scenario* sc, int n_scen, int n_steps
     b->ctas_per_sm = o.ctas_per_sm;
     b->stage = stage;
     b->all_rings = true;
+    b->sq_all = sq_all;
     for (int i = 0; i < n_scen; ++i) b->all_rings = b->all_rings && sc[i].ring != nullptr;
     b->lay = std::move(lay);
     b->work = w;

@@ -70,6 +70,7 @@ struct BatchLaunch {
     Partial* gparts;
     int nscen, ntasks;
     int parity;                    // fields are read from buf[parity], written to buf[parity ^ 1]
+    int sq_all;                    // every scenario has square cells (ax == ay)
     int step0;                     // plan step of this launch's first substep
 };
 
