@@ -120,6 +120,65 @@ class Solver:
         T = self.field.cpu().numpy()
         return T, ring_to_numpy(ring)
 
+    def run_many(self, inputs, plans, outputs, rings_out=None) -> None:
+        """Independent runs streamed through this solver: run i starts from
+        inputs[i] (host (ny, nx) float64 tensors, pinned for overlap), follows
+        plans[i] and leaves its final field in outputs[i] (and its per-step
+        Partials in rings_out[i], host uint8 tensors of 24 bytes per step).
+
+        The copies go on a copy stream through two device staging slots:
+        run i+1's field is copied in, and run i-1's result copied out, while
+        run i computes, so the host link is busy only at the ends of the
+        sequence.  Returns when every output has arrived."""
+        n = len(inputs)
+        if len(plans) != n or len(outputs) != n or (rings_out is not None and len(rings_out) != n):
+            raise ValueError("inputs, plans and outputs must have the same length")
+        if n == 0:
+            return
+        dev = self.device
+        comp = torch.cuda.current_stream(dev)
+        copy = torch.cuda.Stream(device=dev)
+        shape = (self.ny, self.nx)
+        s_in = [torch.empty(shape, dtype=torch.float64, device=dev) for _ in range(2)]
+        s_out = [torch.empty(shape, dtype=torch.float64, device=dev) for _ in range(2)]
+        rings = [self.new_ring(max(len(p) for p in plans) or 1) for _ in range(2)]
+        ev = lambda: torch.cuda.Event()                               # noqa: E731
+        in_ready = [ev() for _ in range(n)]      # staging slot filled (copy stream)
+        in_free = [ev() for _ in range(n)]       # staging slot consumed (compute stream)
+        out_ready = [ev() for _ in range(n)]     # result staged (compute stream)
+        out_free = [ev() for _ in range(n)]      # result copied out (copy stream)
+
+        def copy_in(i):
+            with torch.cuda.stream(copy):
+                if i >= 2:
+                    copy.wait_event(in_free[i - 2])
+                s_in[i % 2].copy_(torch.as_tensor(inputs[i]).reshape(shape), non_blocking=True)
+                in_ready[i].record(copy)
+
+        def copy_out(i):
+            with torch.cuda.stream(copy):
+                copy.wait_event(out_ready[i])
+                outputs[i].copy_(s_out[i % 2], non_blocking=True)
+                if rings_out is not None:
+                    rings_out[i].copy_(rings[i % 2][:rings_out[i].numel()], non_blocking=True)
+                out_free[i].record(copy)
+
+        copy_in(0)
+        for i in range(n):
+            if i + 1 < n:
+                copy_in(i + 1)
+            comp.wait_event(in_ready[i])
+            self.bufs[self.cur].copy_(s_in[i % 2])
+            in_free[i].record(comp)
+            if i >= 2:
+                comp.wait_event(out_free[i - 2])
+            self.advance(plans[i], rings[i % 2])
+            s_out[i % 2].copy_(self.field)
+            out_ready[i].record(comp)
+            copy_out(i)
+        torch.cuda.current_stream(dev).wait_stream(copy)
+        torch.cuda.synchronize(dev)
+
 
 class SolverF32K:
     """The FP32 compensated field (hi + lo f32 pairs) with the same plan API

@@ -367,3 +367,27 @@ def test_square_and_rectangular_cells(gpu):
         assert np.array_equal(b.field(i).cpu().numpy().view(np.uint64), T.view(np.uint64))
         assert b.ring(i)[:n].tobytes() == ring.tobytes()
     b.close()
+
+
+def test_run_many_streams_independent_runs(gpu):
+    """Solver.run_many: each run equals its own advance from its own host
+    field, whatever the overlap of the copies."""
+    torch = torch_mod()
+    from hedgehog_lpbf_b200.solver import ring_to_numpy
+    mat, pr, dom, k = bench_const(300, 260)
+    rng = np.random.default_rng(11)
+    n_runs, n = 4, 7
+    ins = [torch.tensor(300.0 + rng.uniform(0.0, 1500.0, size=(260, 300))).pin_memory()
+           for _ in range(n_runs)]
+    plans = [PL.raster_for_steps(dom, k.dt, n, V=1.0, hatch=100e-6, n_tracks=2, angle=0.3 * i)
+             for i in range(n_runs)]
+    outs = [torch.empty((260, 300), dtype=torch.float64).pin_memory() for _ in range(n_runs)]
+    rings = [torch.empty(24 * n, dtype=torch.uint8).pin_memory() for _ in range(n_runs)]
+    s = solver(k, Tm=mat.Tm, depth=3)
+    s.run_many(ins, plans, outs, rings)
+    for i in range(n_runs):
+        ref = solver(k, Tm=mat.Tm, depth=3, T0=ins[i].numpy())
+        r = ref.new_ring(n)
+        T = ref.advance(plans[i], r).cpu().numpy()
+        assert np.array_equal(outs[i].numpy().view(np.uint64), T.view(np.uint64)), i
+        assert rings[i].numpy().tobytes() == ring_to_numpy(r).tobytes(), i
