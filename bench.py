@@ -512,7 +512,10 @@ def run_b200_arm(args, rank, world, local_rank):
         del sk, T64
 
     del s
-    sh = sharded_leg(args, dev, rank, world, value / world) if args.sharded else None
+    # across ranks only on request: that path (NCCL halo exchange) is
+    # exercised by the tests with gloo ranks on CPU, not on several GPUs
+    run_sh = args.sharded and (world == 1 or args.shard_ranks)
+    sh = sharded_leg(args, dev, rank, world, value / world) if run_sh else None
     pm = None
     if args.process_map:
         pm = process_map_leg(args, dev, rank, world)
@@ -578,6 +581,8 @@ def main():
     ap.add_argument("--no-sharded", dest="sharded", action="store_false",
                     help="skip the row-strip sharded leg")
     ap.add_argument("--sh-steps", type=int, default=300)
+    ap.add_argument("--shard-ranks", action="store_true",
+                    help="with --gpus > 1: also shard one field across the ranks")
     ap.add_argument("--pm-scenarios", type=int, default=256)
     ap.add_argument("--pm-steps", type=int, default=5000)
     ap.add_argument("--no-superstep", dest="superstep", action="store_false",
