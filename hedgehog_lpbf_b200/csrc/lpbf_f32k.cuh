@@ -187,7 +187,10 @@ struct FkStrip {
                 st = stages + sidx * FK_STAGE_FLOATS;
             }
             if constexpr (REDUCE) set_thresholds();
-            const bool fast = !edge && j - K >= 1 && j + 1 <= ny - 2 &&
+            // mirror-edge strips too: row_update patches the edge cells'
+            // outer neighbours itself (nx a multiple of 4: whole lanes)
+            const bool fast = (!edge || (p.c.bc == 0 && (p.c.nx & 3) == 0)) &&
+                              j - K >= 1 && j + 1 <= ny - 2 &&
                               (!src_strip || j + 1 < p.band_lo || j - K > p.band_hi);
             if (fast && j < jend) {
                 fast_row<0>(j, st);
