@@ -173,6 +173,8 @@ struct FkStrip {
             for (int b = 0; b < pre; ++b) issue(b);
         }
         const int jlast = y1 - 1 + K;
+        // per-box thresholds change only when an exact pass moves a peak
+        if constexpr (REDUCE) set_thresholds();
         for (int b = 0, j = jy0; j <= jlast && !failed; ++b, j += ADV_R) {
             const float* st = nullptr;
             if (j < jend) {
@@ -186,7 +188,6 @@ struct FkStrip {
                 }
                 st = stages + sidx * FK_STAGE_FLOATS;
             }
-            if constexpr (REDUCE) set_thresholds();
             // mirror-edge strips too: row_update patches the edge cells'
             // outer neighbours itself (nx a multiple of 4: whole lanes)
             const bool fast = (!edge || (p.c.bc == 0 && (p.c.nx & 3) == 0)) &&
@@ -460,6 +461,7 @@ struct FkStrip {
             exact_level(t, j);
             __syncwarp();
         }
+        set_thresholds();
     }
 };
 
