@@ -33,11 +33,11 @@ FkCoef make_fk(const Coef& c, double T_edge) {
     return f;
 }
 
-template <int K, bool REDUCE>
+template <int K, bool REDUCE, bool SQ>
 cudaError_t launch_fk(const float* hi_in, const float* lo_in, float* hi_out, float* lo_out,
                       const Coef& c, const FkCoef& f, const LaserSub* las, Partial* ring,
                       Workspace* ws, int rows, cudaStream_t stream) {
-    auto kern = advance_f32k_kernel<K, REDUCE>;
+    auto kern = advance_f32k_kernel<K, REDUCE, SQ>;
     static int occ[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -97,10 +97,19 @@ cudaError_t launch_fk_k(int K, bool reduce, const float* hi_in, const float* lo_
                         float* hi_out, float* lo_out, const Coef& c, const FkCoef& f,
                         const LaserSub* las, Partial* ring, Workspace* ws, int rows,
                         cudaStream_t s) {
-#define LPBF_FK(KK)                                                                        \
-    case KK:                                                                               \
-        return reduce ? launch_fk<KK, true>(hi_in, lo_in, hi_out, lo_out, c, f, las, ring, ws, rows, s) \
-                      : launch_fk<KK, false>(hi_in, lo_in, hi_out, lo_out, c, f, las, ring, ws, rows, s);
+    // square cells (the f32 coefficients equal) take the one-Laplacian form
+    const bool sq = f.ax == f.ay;
+#define LPBF_FK(KK)                                                                         \
+    case KK:                                                                                \
+        if (sq)                                                                             \
+            return reduce ? launch_fk<KK, true, true>(hi_in, lo_in, hi_out, lo_out, c, f, las, \
+                                                      ring, ws, rows, s)                    \
+                          : launch_fk<KK, false, true>(hi_in, lo_in, hi_out, lo_out, c, f,  \
+                                                       las, ring, ws, rows, s);             \
+        return reduce ? launch_fk<KK, true, false>(hi_in, lo_in, hi_out, lo_out, c, f, las,  \
+                                                   ring, ws, rows, s)                       \
+                      : launch_fk<KK, false, false>(hi_in, lo_in, hi_out, lo_out, c, f, las, \
+                                                    ring, ws, rows, s);
     switch (K) {
         LPBF_FK(1)
         LPBF_FK(2)

@@ -62,17 +62,30 @@ __device__ __host__ __forceinline__ float fk_pow4(float hi, float lo) {
 }
 
 // One compensated cell update.  (th, tl) centre; neighbour pairs; S_dt the
-// dt-scaled FP64 source rounded to f32.
+// dt-scaled FP64 source rounded to f32.  SQ (ax == ay): one Laplacian of the
+// hi parts plus one of the lo parts, the source and loss in the same fused
+// chain; otherwise the x and y terms apart.  T^4 - Ta^4 is one fused
+// multiply-add.
+template <bool SQ>
 __device__ __forceinline__ void fk_cell(float th, float tl, float Lh, float Ll, float Rh,
                                         float Rl, float Uh, float Ul, float Dh, float Dl,
                                         float S, const FkCoef& f, float& oh, float& ol) {
-    const float lx = ((__fsub_rn(Rh, th) + __fsub_rn(Lh, th)) + ((Rl - tl) + (Ll - tl)));
-    const float ly = ((__fsub_rn(Dh, th) + __fsub_rn(Uh, th)) + ((Dl - tl) + (Ul - tl)));
-    const float inc = fmaf(f.ax, lx, __fmul_rn(f.ay, ly));
     const float da = __fsub_rn(th, f.Ta_hi) + (tl - f.Ta_lo);
-    const float e4 = __fsub_rn(fk_pow4(th, tl), f.Ta4);
+    const float t = th + tl;
+    const float t2 = t * t;
+    const float e4 = fmaf(t2, t2, -f.Ta4);
     const float loss = fmaf(f.crad, e4, __fmul_rn(f.cls, da));
-    const float d = __fsub_rn(__fadd_rn(inc, S), loss);
+    float d;
+    if constexpr (SQ) {
+        const float lh = (__fsub_rn(Rh, th) + __fsub_rn(Lh, th)) +
+                         (__fsub_rn(Dh, th) + __fsub_rn(Uh, th));
+        const float ll = fmaf(-4.0f, tl, (Rl + Ll) + (Dl + Ul));
+        d = fmaf(f.ax, lh + ll, __fsub_rn(S, loss));
+    } else {
+        const float lx = ((__fsub_rn(Rh, th) + __fsub_rn(Lh, th)) + ((Rl - tl) + (Ll - tl)));
+        const float ly = ((__fsub_rn(Dh, th) + __fsub_rn(Uh, th)) + ((Dl - tl) + (Ul - tl)));
+        d = fmaf(f.ax, lx, fmaf(f.ay, ly, __fsub_rn(S, loss)));
+    }
     // two-sum of th + d, remainder folded into lo, then renormalised
     const float s = __fadd_rn(th, d);
     const float bp = __fsub_rn(s, th);
@@ -87,7 +100,7 @@ __device__ __forceinline__ bool fk_gt(float ah, float al, float bh, float bl) {
     return ah > bh || (ah == bh && al > bl);
 }
 
-template <int K, bool REDUCE>
+template <int K, bool REDUCE, bool SQ>
 struct FkStrip {
     static constexpr int V = ADV_V;
 
@@ -257,7 +270,7 @@ struct FkStrip {
         }
 #pragma unroll
         for (int v = 0; v < V; ++v)
-            fk_cell(ch[v], cl[v], Lh[v], Ll[v], Rh[v], Rl[v], uh[v], ul[v], dh[v], dl[v],
+            fk_cell<SQ>(ch[v], cl[v], Lh[v], Ll[v], Rh[v], Rl[v], uh[v], ul[v], dh[v], dl[v],
                     S ? S[v] : 0.0f, p.f, oh[v], ol[v]);
     }
 
@@ -465,7 +478,7 @@ struct FkStrip {
     }
 };
 
-template <int K, bool REDUCE>
+template <int K, bool REDUCE, bool SQ>
 __global__ void __launch_bounds__(ADV_WARPS * 32, AdvOcc<K>::min_ctas)
 advance_f32k_kernel(const __grid_constant__ CUtensorMap map_hi,
                     const __grid_constant__ CUtensorMap map_lo,
@@ -489,7 +502,7 @@ advance_f32k_kernel(const __grid_constant__ CUtensorMap map_hi,
     }
     __syncwarp();
 
-    FkStrip<K, REDUCE> ws(p, &map_hi, &map_lo, stages, bars, lane, s_tmx[wid], s_arg[wid],
+    FkStrip<K, REDUCE, SQ> ws(p, &map_hi, &map_lo, stages, bars, lane, s_tmx[wid], s_arg[wid],
                           s_ymn[wid], s_ymx[wid], s_box[wid]);
     for (;;) {
         unsigned int t = 0;

@@ -113,3 +113,17 @@ def test_f32k_substrate_temperature_differs_from_ambient(gpu):
     T, ring, _ = _run_f32k(k, plan, T0, Tm=mat.Tm)
     assert float(np.max(np.abs(T - T_ref))) <= ATOL_K
     assert float(np.max(np.abs(ring["tmax"] - ring_ref["tmax"]))) <= ATOL_K
+
+
+def test_f32k_rectangular_cells_within_0p05K(gpu):
+    """dy != dx: the two-term Laplacian form of the compensated update."""
+    mat, pr = P.benchmark_material_process()
+    dom = P.Domain(Lx=255 * 5e-6, Ly=199 * 6.5e-6, nx=256, ny=200)
+    k = P.make_const(mat, pr, dom, P.dt_fraction(mat, dom))
+    assert k.inv_dx2 != k.inv_dy2
+    T0 = np.full(256 * 200, 300.0)
+    plan = PL.raster_for_steps(dom, k.dt, 400, V=1.0, hatch=100e-6, n_tracks=2, angle=0.5)
+    T_ref, ring_ref = O.run(T0, k, PL.laser_array(plan), Tm=mat.Tm)
+    T, ring, _ = _run_f32k(k, plan, T0, Tm=mat.Tm)
+    assert float(np.max(np.abs(T - T_ref))) <= ATOL_K
+    assert float(np.max(np.abs(ring["tmax"] - ring_ref["tmax"]))) <= ATOL_K
