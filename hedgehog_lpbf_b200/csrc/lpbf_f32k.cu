@@ -59,8 +59,12 @@ cudaError_t launch_fk(const float* hi_in, const float* lo_in, float* hi_out, flo
     for (int t = 0; t < K; ++t) p.las[t] = las[t];
     laser_band(c, las, K, &p.band_lo, &p.band_hi, &p.bandx_lo, &p.bandx_hi);
     p.nstrips = (c.nx + ADV_WOUT - 1) / ADV_WOUT;
-    // 24-row tasks measured best here (taller ones lost about 3 %)
-    p.H = std::max(std::min(rows > 0 ? rows : 24, c.ny), 1);
+    int H = rows;
+    if (H <= 0) {   // about three tasks per resident warp, 12..48 rows (48 measured best)
+        const long long want = (long long)c.ny * p.nstrips / (3ll * resident * ADV_WARPS);
+        H = (int)std::max(12ll, std::min(48ll, want));
+    }
+    p.H = std::max(std::min(H, c.ny), 1);
     // rows whose tasks (owned rows +- K) reach the source band: 8-row tasks
     p.Hb = p.H;
     if (p.band_lo <= p.band_hi) {
