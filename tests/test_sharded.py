@@ -133,15 +133,15 @@ def _free_port():
     return p
 
 
-def _worker(rank, world, port, out):
+def _worker(rank, world, port, out, depth=3, bc=0):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         mat, k, T0, las, plan = _case()
-        f = S.ShardedField.distributed(k, rank, world, depth=3, device="cpu", T0=T0,
-                                       stepper=OracleStripStepper(Tm=mat.Tm))
+        f = S.ShardedField.distributed(k, rank, world, depth=depth, device="cpu", T0=T0,
+                                       stepper=OracleStripStepper(bc=bc, Tm=mat.Tm))
         rings = f.advance(plan)
         # every rank takes the same collective steps in the same order
         T = f.field().numpy()
@@ -228,3 +228,22 @@ def test_gpu_advance_rows_rejects_bad_windows(gpu):
     assert call(15, 3, 23, 3) == -1                       # strip beyond the field
     assert call(7, 3, 23, 3, phys=1) == -2                # baseline physics only
     del opts
+
+
+def test_three_gloo_ranks_interior_strip():
+    """An interior strip trades rows with both neighbours; fixed edges, 2 steps
+    per launch."""
+    import torch.multiprocessing as mp
+    from oracle import oracle as O
+    world = 3
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_worker, args=(world, _free_port(), out, 2, 1), nprocs=world,
+                       start_method="spawn", join=True)
+    mat, k, T0, las, plan = _case()
+    T_ref, ring_ref = O.run(T0.ravel(), k, las, bc=1, T_D=300.0, Tm=mat.Tm)
+    mid = out[1][2]
+    assert mid.top == mid.bot == 2
+    for r in range(world):
+        T, pb, _ = out[r]
+        _check(T.ravel(), np.frombuffer(pb, dtype=PARTIAL_DTYPE), T_ref, ring_ref)
