@@ -11,8 +11,9 @@
 //     so the Laplacian keeps ~48 significant bits;
 //   * the loss terms and the increment are f32; the Gaussian source is
 //     evaluated in FP64 (as in the FP64 path) and rounded once;
-//   * the increment is added with an error-free two-sum, and the rounding
-//     error is carried in lo (Kahan-compensated accumulation).
+//   * the increment is added with an error-free sum (Fast2Sum: the
+//     increment is never larger than T), and the rounding error is carried
+//     in lo (Kahan-compensated accumulation).
 // Memory traffic per cell-update equals the FP64 path's (hi + lo = 8 bytes).
 //
 // Structure (warp tasks, lanes, TMA pipeline, wavefront, fast/general boxes,
@@ -86,10 +87,11 @@ __device__ __forceinline__ void fk_cell(float th, float tl, float Lh, float Ll, 
         const float ly = ((__fsub_rn(Dh, th) + __fsub_rn(Uh, th)) + ((Dl - tl) + (Ul - tl)));
         d = fmaf(f.ax, lx, fmaf(f.ay, ly, __fsub_rn(S, loss)));
     }
-    // two-sum of th + d, remainder folded into lo, then renormalised
+    // th + d with its rounding error (Fast2Sum, exact for |d| <= |th|: a
+    // step's increment is far smaller than the temperature), the error
+    // folded into lo, then renormalised
     const float s = __fadd_rn(th, d);
-    const float bp = __fsub_rn(s, th);
-    const float err = __fadd_rn(__fsub_rn(th, __fsub_rn(s, bp)), __fsub_rn(d, bp));
+    const float err = __fsub_rn(d, __fsub_rn(s, th));
     const float lo = __fadd_rn(tl, err);
     oh = __fadd_rn(s, lo);
     ol = __fsub_rn(lo, __fsub_rn(oh, s));
