@@ -478,13 +478,12 @@ struct WarpStrip {
             } else {
                 st_global_v4_pred(p.Tout + (size_t)r * p.c.nx + xl, nv, owned_row && own_all);
             }
-            // Only owned rows are tested: the first halo rows of a task are
+            // Only owned rows are tested (an infinite threshold elsewhere, so
+            // no branch splits the box): the first halo rows of a task are
             // computed from window slots that still hold the warp's previous
             // task (values of no use here, which would only trigger empty
             // exact passes).
-            if constexpr (REDUCE) {
-                if (owned_row) row_stats<T - 1, P>(r, nv, own_all, true);
-            }
+            if constexpr (REDUCE) row_stats_fast<T - 1, P>(nv, owned_row);
             fast_level<P, T + 1, SQ>(jj);
         }
     }
@@ -665,6 +664,25 @@ struct WarpStrip {
         hit[T] = hit[T] | rh;
         if constexpr (T == K - 1) {
             if (rh && own) {
+                double2* d = reinterpret_cast<double2*>(&rs->box[P][lane][0]);
+                d[0] = make_double2(nv[0], nv[1]);
+                d[1] = make_double2(nv[2], nv[3]);
+                kmask |= 1u << P;
+            }
+        }
+    }
+
+    // The fast body's test: whole lanes, rows outside the task's own rows
+    // against an infinite threshold.
+    template <int T, int P>
+    __device__ __forceinline__ void row_stats_fast(const double* nv, bool owned_row) {
+        const double th = owned_row ? thr[T] : INFINITY;
+        bool rh = false;
+#pragma unroll
+        for (int v = 0; v < V; ++v) rh = rh | !(nv[v] <= th);
+        hit[T] = hit[T] | rh;
+        if constexpr (T == K - 1) {
+            if (rh && own_all && owned_row) {
                 double2* d = reinterpret_cast<double2*>(&rs->box[P][lane][0]);
                 d[0] = make_double2(nv[0], nv[1]);
                 d[1] = make_double2(nv[2], nv[3]);
