@@ -32,6 +32,16 @@ constexpr size_t FK_SMEM_BYTES =
     size_t(ADV_WARPS) * ADV_S * FK_STAGE_FLOATS * sizeof(float)
     + size_t(ADV_WARPS) * ADV_S * sizeof(uint64_t);
 
+// 16-byte store issued under a predicate (no branch).  It carries a
+// "memory" clobber: the exact reduction reads level-K values back from the
+// output field, and those loads must stay after the stores.
+__device__ __forceinline__ void st_global_v4f_pred(float* p, const float* v, bool pred) {
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %5, 0;\n\t"
+                 "@q st.global.v4.f32 [%0], {%1, %2, %3, %4};\n\t}"
+                 :: "l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "r"((int)pred)
+                 : "memory");
+}
+
 struct FkCoef {
     float ax, ay, cls, crad;
     float Ta_hi, Ta_lo, Ta4;       // linear-loss reference T as a pair; Ta4 = f4(Tamb)
@@ -363,17 +373,13 @@ struct FkStrip {
 #pragma unroll
             for (int v = 0; v < V; ++v) { bh[SC][v] = oh[v]; bl[SC][v] = ol[v]; }
         } else {
-            if (owned_row && owned_lane()) {
-                const size_t off = (size_t)r * p.c.nx + xl;
-                if (xl + V <= p.c.nx) {
-                    *reinterpret_cast<float4*>(p.Thi_out + off) = make_float4(oh[0], oh[1], oh[2], oh[3]);
-                    *reinterpret_cast<float4*>(p.Tlo_out + off) = make_float4(ol[0], ol[1], ol[2], ol[3]);
-                } else {
-#pragma unroll
-                    for (int v = 0; v < V; ++v)
-                        if (xl + v < p.c.nx) { p.Thi_out[off + v] = oh[v]; p.Tlo_out[off + v] = ol[v]; }
-                }
-            }
+            // nx is a multiple of 4 (checked on entry): an owned lane's four
+            // cells are in the field and 16-byte aligned; the stores are
+            // predicated, so no branch splits the box
+            const size_t off = (size_t)r * p.c.nx + xl;
+            const bool st = owned_row && owned_lane();
+            st_global_v4f_pred(p.Thi_out + off, oh, st);
+            st_global_v4f_pred(p.Tlo_out + off, ol, st);
         }
         if constexpr (REDUCE) {
             bool h = hit[T - 1];
