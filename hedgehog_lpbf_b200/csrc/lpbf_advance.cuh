@@ -26,13 +26,15 @@
 // go straight to HBM as 32-byte stores.
 //
 // Fast and general boxes.  A box whose rows, over all K levels, are interior
-// to the domain, carry no source and lie in a strip away from the x edges
-// runs a branch-free body; rows of the chunk's own halo are computed there
-// too and only masked out of the store and the reduction (a value outside a
-// level's valid range only ever feeds rows that are themselves outside the
-// next level's range).  Every other box runs the general body, which handles
-// domain edges, fixed-value boundaries, partial ownership and the Gaussian
-// source (evaluated out of line, so exp is not replicated).  Both bodies evaluate
+// to the domain and carry no source runs a branch-free body, in strips away
+// from the x edges and in strips at a mirror x edge alike (there the lane
+// just off the field holds its neighbour's cells in reverse order); rows of
+// the chunk's own halo are computed there too and only masked out of the
+// store and the reduction (a value outside a level's valid range only ever
+// feeds rows that are themselves outside the next level's range).  Every
+// other box runs the general body, which handles the top and bottom edges,
+// fixed-value boundaries, partial ownership and the Gaussian source
+// (evaluated out of line, so exp is not replicated).  Both bodies evaluate
 // every cell with the same function, so results depend neither on the body
 // nor on K, H or the task order.
 //
