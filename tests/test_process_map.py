@@ -143,3 +143,18 @@ def test_process_map_cli_rejects_bad_arguments():
         PM.main(["--scenarios", "0"])
     with pytest.raises(SystemExit):
         PM.main(["--rows", "1,2", "--depth", "2", "--steps", "0"])
+
+
+@pytest.mark.gpu
+def test_process_map_cli_runs_and_writes_csv(gpu, tmp_path):
+    out = tmp_path / "pm.csv"
+    rc = PM.main(["--scenarios", "2", "--steps", "6", "--side", "256", "--depth", "2",
+                  "--rows", "12,12,12,12", "--out", str(out)])
+    assert rc == 0
+    lines = out.read_text().strip().splitlines()
+    assert lines[0].split(",") == list(PM.COLUMNS)
+    assert len(lines) == 3
+    for line in lines[1:]:
+        row = dict(zip(PM.COLUMNS, line.split(",")))
+        assert int(row["side"]) == 256 and int(row["steps"]) == 6
+        assert float(row["peak_T_K"]) > 300.0
