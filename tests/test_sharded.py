@@ -247,3 +247,29 @@ def test_three_gloo_ranks_interior_strip():
     for r in range(world):
         T, pb, _ = out[r]
         _check(T.ravel(), np.frombuffer(pb, dtype=PARTIAL_DTYPE), T_ref, ring_ref)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_strip_partials_combine_to_the_field_reduction(seed):
+    """Random fields with planted ties and molten rows, cut into random strip
+    counts: per-strip Partials (owned rows, field numbering) combined by the
+    reduction rule equal the oracle's whole-field reduction."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(seed)
+    nx, ny = int(rng.integers(4, 40)), int(rng.integers(6, 60))
+    Tm = 1500.0
+    T = rng.choice([300.0, 900.0, 1600.0, 2000.0], size=(ny, nx), p=[0.6, 0.25, 0.1, 0.05])
+    if seed % 2:
+        T[:] = 300.0                                    # all tied, none molten
+    parts = int(rng.integers(1, min(6, ny) + 1))
+    rings = []
+    for s in S.strip_layout(ny, parts, 1):
+        own = T[s.a:s.b]
+        tm, ag, mn, mx = O.reduce(own.ravel(), nx, s.b - s.a, Tm)
+        r = np.zeros(1, dtype=PARTIAL_DTYPE)
+        neutral = ag >= nx * (s.b - s.a)
+        r[0] = (tm, nx * ny if neutral else ag + s.a * nx,
+                ny if mx < 0 else mn + s.a, -1 if mx < 0 else mx + s.a)
+        rings.append(r)
+    got = S.combine_partials(rings, nx, ny)[0]
+    assert tuple(got) == O.reduce(T.ravel(), nx, ny, Tm)
