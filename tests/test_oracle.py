@@ -160,3 +160,27 @@ def test_reference_steptiletask_matches_oracle_when_built():
     T_o, ring = O.run(T0, k, las, Tm=mat.Tm)
     assert np.array_equal(T_hh, T_o)
     assert np.array_equal(trace, ring["tmax"])
+
+
+@pytest.mark.parametrize("seed", range(5))
+def test_reference_cpu_step_matches_oracle_random_cases(seed):
+    """Random grids, spot paths, start fields and substrate temperatures
+    (Tsub != Tamb included): the oracle equals the live reference bit for
+    bit."""
+    if not O.have_reference():
+        pytest.skip("oracle/_ref not built here")
+    rng = np.random.default_rng(100 + seed)
+    nx, ny = int(rng.integers(8, 90)), int(rng.integers(4, 60))
+    mat, pr = P.benchmark_material_process(P=float(rng.uniform(100, 400)),
+                                           r0=float(rng.uniform(30e-6, 70e-6)))
+    pr.Tsub = float(rng.choice([pr.Tamb, 420.0, 250.0]))
+    pr.radiation = bool(seed % 2 == 0)
+    dom = P.Domain(Lx=(nx - 1) * 5e-6, Ly=(ny - 1) * 5e-6, nx=nx, ny=ny)
+    k = P.make_const(mat, pr, dom, P.dt_fraction(mat, dom))
+    T0 = 300.0 + rng.uniform(0, 2500, size=nx * ny)
+    n = int(rng.integers(3, 12))
+    las = np.stack([rng.uniform(-0.1, 1.1, n) * dom.Lx, rng.uniform(-0.1, 1.1, n) * dom.Ly,
+                    rng.choice([0.0, 0.5, 1.0], n)], axis=1)
+    T_o, _ = O.run(T0, k, las, with_ring=False)
+    T_r = O.ref_run_plan(T0, k, las)
+    assert np.array_equal(T_o, T_r)
