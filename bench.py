@@ -77,16 +77,14 @@ def measured_peaks():
     return 6650.0, "fallback (no MEASURED_PEAKS.json: earlier copy-bandwidth measurement on B200)"
 
 
-def profile_traffic(depth):
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
-    summary (profiles/advance_kernel_8192.md), or None."""
-    p = os.path.join(ROOT, "profiles", "advance_kernel_8192.md")
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.startswith(f"traffic_per_launch_bytes_depth{depth}"):
-            return float(line.split("=")[1].split()[0])
-    return None
+# ncu counters of one full-size launch of the dominant kernel (8192^2, depth
+# 3, the bench's own command), summarised with the command that produced
+# them in profiles/advance_kernel_8192.md.  Per launch: DRAM bytes read +
+# written, and the FP64 pipe's share of active cycles.
+ADVANCE_PROFILE = {
+    3: {"dram_bytes": None, "fp64_pipe": None, "launch_us": None,
+        "source": "profiles/advance_kernel_8192.md"},
+}
 
 
 class ClockSampler:
@@ -174,6 +172,48 @@ def cpu_reference_rate(mat, pr, dom, k, plan, budget_s: float, threads: int | No
             "sample": desc, "wall_s": wall}
 
 
+def cpu_single_thread_rate(mat, pr, dom, k, budget_s: float):
+    """The reference's single-thread CPU solver, run_cpu (src/gpu/lpbf_cuda.cu:
+    423-448: cpu_step plus measure_host every step), on the same grid and
+    constants.  It follows its built-in single-track law rather than the
+    raster; its per-step work does not depend on the laser's path (the
+    source is evaluated at every cell)."""
+    from oracle import oracle as O
+    if not O.have_reference():
+        return None
+    w1 = O.ref_run_cpu(mat, pr, dom, k.dt, 1)["wall_ms"] * 1e-3
+    n = int(max(1, budget_s / max(w1, 1e-3)))
+    wall = O.ref_run_cpu(mat, pr, dom, k.dt, n)["wall_ms"] * 1e-3
+    return {"value": dom.nx * dom.ny * n / wall / 1e9, "unit": "GCell-updates/s", "cores": 1,
+            "kind": "reference", "wall_s": wall,
+            "sample": f"reference run_cpu (single thread, its single-track law), {n} steps of "
+                      f"{dom.nx}x{dom.ny}"}
+
+
+def reference_gpu_rate(mat, pr, dom, k, plan, n1: int = 192, n2: int = 1216):
+    """The reference's own GPU path on this GPU: its GpuStepTask graph
+    (include/gpu_step_task.hpp, run as run_one_row does, hh_gpu_main.cpp:171-
+    207) with its kernels (src/gpu/kernels.cu built for sm_100a), default
+    options (mode 2, batch 64, unfused, pageable staging) and with the fused
+    step+reduce kernel, over the bench's raster plan.  Steady-state rate from
+    two run lengths (the task's device set-up cancels in the difference)."""
+    from oracle import oracle as O
+    if not O.have_reference():
+        return None
+    out = {"unit": "GCell-updates/s", "kind": "reference",
+           "what": "reference GpuStepTask graph (mode 2, batch 64) with its own kernels "
+                   "(kernels.cu built for sm_100a), wall clock, "
+                   f"({n2} - {n1}) steps of {dom.nx}x{dom.ny} on the bench's raster"}
+    for name, fused in (("unfused", False), ("fused", True)):
+        O.ref_gpu_task_run(k, dom, plan[:64], mat.Tm, pr.Tamb, fused=fused)     # warm-up
+        t1, _ = O.ref_gpu_task_run(k, dom, plan[:n1], mat.Tm, pr.Tamb, fused=fused)
+        t2, pk = O.ref_gpu_task_run(k, dom, plan[:n2], mat.Tm, pr.Tamb, fused=fused)
+        out[name] = {"value": dom.nx * dom.ny * (n2 - n1) / ((t2 - t1) * 1e-3) / 1e9,
+                     "ms_per_step": (t2 - t1) / (n2 - n1), "peak_T_K": pk}
+    out["value"] = max(out["unfused"]["value"], out["fused"]["value"])
+    return out
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -194,6 +234,17 @@ def run_reference_arm(args, rank, world):
             "impl": "reference", "config": config(None, args.gpus), "cpu_baseline": cb,
             "e2e": {"value": rate, "unit": "GCell-updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    st = cpu_single_thread_rate(mat, pr, dom, k, budget_s=args.ref_budget)
+    if st:
+        cb["single_thread_run_cpu"] = st
+    try:
+        import torch
+        have_gpu = torch.cuda.is_available()
+    except Exception:
+        have_gpu = False
+    if have_gpu and N_SIDE == 8192 and not args.no_ref_gpu:
+        # beside the CPU figure: the reference's own GPU task graph on this GPU
+        line["ref_gpu"] = reference_gpu_rate(mat, pr, dom, k, plan)
     print(json.dumps(line), flush=True)
 
 
@@ -529,7 +580,25 @@ def run_b200_arm(args, rank, world, local_rank):
     launch_ms = statistics.median(step_ms) / launches
     steps_per_launch = STEPS_PER_ITER / launches
     achieved = BYTES_PER_UPDATE * cells * steps_per_launch / (launch_ms * 1e-3) / 1e9
-    traffic = profile_traffic(depth)
+    prof = ADVANCE_PROFILE.get(depth, {}) if N_SIDE == 8192 else {}
+    traffic = prof.get("dram_bytes")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                "kernel": f"advance_kernel<{depth},TMA,reduce>",
+                "algorithmic_bytes": f"{BYTES_PER_UPDATE} B per cell-update x {cells} cells"
+                                     f" x {steps_per_launch:g} steps per launch",
+                "frac_meaning": "algorithmic bytes of the time steps one launch advances "
+                                "(temporal blocking: effective, may exceed 1)",
+                "launch_ms": launch_ms}
+    if traffic:
+        # the DRAM bytes ncu counted for one launch over this run's launch time
+        roofline["dram_gbs"] = traffic / (launch_ms * 1e-3) / 1e9
+        roofline["dram_frac"] = roofline["dram_gbs"] / peak
+    if prof.get("fp64_pipe") is not None:
+        roofline["fp64_pipe"] = prof["fp64_pipe"]
+        roofline["limiter"] = prof.get("limiter")
+    if prof:
+        roofline["profile"] = prof["source"]
     line = {
         "metric": "GCell-updates/s", "value": value, "unit": "GCell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -537,13 +606,7 @@ def run_b200_arm(args, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (uniform 300 K start, seeded raster plan per rank)",
         "config": config(depth, world),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": peak_src,
-                     "kernel": f"advance_kernel<{depth},TMA,reduce>",
-                     "algorithmic_bytes": f"{BYTES_PER_UPDATE} B per cell-update x {cells} cells"
-                                          f" x {steps_per_launch:g} steps per launch",
-                     "launch_ms": launch_ms},
+        "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": "GCell-updates/s",
                 "h2d_bytes_per_step": cells * 8,
                 "d2h_bytes_per_step": cells * 8 + STEPS_PER_ITER * 24,
@@ -559,7 +622,21 @@ def run_b200_arm(args, rank, world, local_rank):
         "error_word": err,
     }
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_reference_rate(mat, pr, dom, k, plan, budget_s=args.ref_budget)
+        # the reference's own implementations of the step, timed here as the
+        # baselines: its multi-threaded CPU task, its single-thread run_cpu
+        # and its GPU task graph on this GPU
+        cb = cpu_reference_rate(mat, pr, dom, k, plan, budget_s=args.ref_budget)
+        st = cpu_single_thread_rate(mat, pr, dom, k, budget_s=args.ref_budget)
+        if st:
+            cb["single_thread_run_cpu"] = st
+        line["cpu_baseline"] = cb
+        if N_SIDE == 8192 and not args.no_ref_gpu:
+            torch.cuda.empty_cache()
+            rg = reference_gpu_rate(mat, pr, dom, k, plan)
+            if rg:
+                line["ref_gpu"] = rg
+                line["speedup_vs_ref_gpu"] = value / rg["value"]
+                line["e2e_speedup_vs_ref_gpu"] = e2e_value / rg["value"]
     print(json.dumps(line), flush=True)
 
 
@@ -573,7 +650,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--ref-budget", type=float, default=15.0,
                     help="seconds of CPU work per reference sample")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the reference baselines (CPU and GPU)")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the reference GPU task graph baseline")
     ap.add_argument("--no-f32k", dest="f32k", action="store_false",
                     help="skip the FP32 compensated leg")
     ap.add_argument("--no-process-map", dest="process_map", action="store_false",

@@ -96,7 +96,8 @@ SIGNATURES = {
     "lpbf_b200_f32k_join": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, _vp]),
     "lpbf_b200_advance_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(StepConst), _vp,
                                                  ctypes.c_int, ctypes.POINTER(Opts), _vp, _vp,
-                                                 ctypes.POINTER(ctypes.c_int)]),
+                                                 ctypes.POINTER(ctypes.c_int),
+                                                 ctypes.POINTER(ctypes.c_uint)]),
     "lpbf_b200_batch_size_class": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
     "lpbf_b200_batch_workspace_bytes": (ctypes.c_size_t, [_sp, ctypes.c_int, ctypes.c_int, _bop]),
     "lpbf_b200_batch_create": (ctypes.c_int, [_sp, ctypes.c_int, ctypes.c_int, _bop, _vp,

@@ -124,7 +124,7 @@ namespace {
 template <int K, bool TMA, bool REDUCE, bool SQ>
 cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const LaserSub* las,
                      Partial* ring, Workspace* ws, Partial* ref_out, long long ref_nparts,
-                     int rows, cudaStream_t stream, const RowWindow* win) {
+                     int rows, cudaStream_t stream, const RowWindow* win, int parts_cap) {
     auto kern = advance_kernel<K, TMA, REDUCE, SQ>;
     const size_t smem = TMA ? ADV_SMEM_BYTES : 0;
 
@@ -201,9 +201,11 @@ cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const Laser
     p.nchunks = p.nA + p.nB + (p.row_hi - p.Yb + p.H - 1) / p.H;
     p.ntasks = p.nstrips * p.nchunks;
     int grid = std::min((p.ntasks + ADV_WARPS - 1) / ADV_WARPS, resident);
-    if (REDUCE && !ref_out) grid = std::min(grid, MAX_CTAS);
+    if (REDUCE && !ref_out) grid = std::min(grid, std::min(MAX_CTAS, parts_cap / K));
     if (ref_out) grid = (int)std::min<long long>(grid, ref_nparts);
     grid = std::max(grid, 1);
+    // every CTA of a reducing launch writes K records into ws->parts
+    if (REDUCE && !ref_out && (long long)grid * K > parts_cap) return cudaErrorInvalidValue;
     p.Tin = Tin;
     p.Tout = Tout;
     p.ring = ring;
@@ -227,20 +229,22 @@ cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const Laser
 template <int K, bool SQ>
 cudaError_t launch_k2(bool tma, bool reduce, const double* Tin, double* Tout, const Coef& c,
                       const LaserSub* las, Partial* ring, Workspace* ws, Partial* ref_out,
-                      long long ref_nparts, int rows, cudaStream_t s, const RowWindow* w) {
+                      long long ref_nparts, int rows, cudaStream_t s, const RowWindow* w,
+                      int cap) {
     if (tma) {
         const cudaError_t e = reduce
             ? launch_t<K, true, true, SQ>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows,
-                                          s, w)
+                                          s, w, cap)
             : launch_t<K, true, false, SQ>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows,
-                                           s, w);
+                                           s, w, cap);
         if (e != cudaErrorNotSupported) return e;
         // tensor map unavailable: fall through to the direct-load kernel
     }
     return reduce
-        ? launch_t<K, false, true, SQ>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s, w)
+        ? launch_t<K, false, true, SQ>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s, w,
+                                       cap)
         : launch_t<K, false, false, SQ>(Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, s,
-                                        w);
+                                        w, cap);
 }
 
 // Square cells (ax == ay, the same comparison the kernels make) take the
@@ -248,12 +252,13 @@ cudaError_t launch_k2(bool tma, bool reduce, const double* Tin, double* Tout, co
 template <int K>
 cudaError_t launch_k(bool tma, bool reduce, const double* Tin, double* Tout, const Coef& c,
                      const LaserSub* las, Partial* ring, Workspace* ws, Partial* ref_out,
-                     long long ref_nparts, int rows, cudaStream_t s, const RowWindow* w) {
+                     long long ref_nparts, int rows, cudaStream_t s, const RowWindow* w,
+                     int cap) {
     return c.ax == c.ay
         ? launch_k2<K, true>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows,
-                             s, w)
+                             s, w, cap)
         : launch_k2<K, false>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows,
-                              s, w);
+                              s, w, cap);
 }
 
 }  // namespace
@@ -261,15 +266,15 @@ cudaError_t launch_k(bool tma, bool reduce, const double* Tin, double* Tout, con
 cudaError_t launch_advance(int K, const double* Tin, double* Tout, const Coef& c,
                            const LaserSub* las, Partial* ring, Workspace* ws,
                            Partial* ref_out, long long ref_nparts, int rows,
-                           cudaStream_t stream, const RowWindow* win) {
+                           cudaStream_t stream, const RowWindow* win, int parts_cap) {
     const bool tma = tma_ok(Tin, c.nx) && tma_ok(Tout, c.nx);
     const bool reduce = (ring != nullptr) || (ref_out != nullptr);
     if (reduce && !ref_out && !ws) return cudaErrorInvalidValue;
     switch (K) {
-        case 1: return launch_k<1>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream, win);
-        case 2: return launch_k<2>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream, win);
-        case 3: return launch_k<3>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream, win);
-        case 4: return launch_k<4>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream, win);
+        case 1: return launch_k<1>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream, win, parts_cap);
+        case 2: return launch_k<2>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream, win, parts_cap);
+        case 3: return launch_k<3>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream, win, parts_cap);
+        case 4: return launch_k<4>(tma, reduce, Tin, Tout, c, las, ring, ws, ref_out, ref_nparts, rows, stream, win, parts_cap);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -87,12 +87,15 @@ inline bool tma_ok(const void* p, int nx) {
 //   ref_out: reference fused-reduce layout (K == 1 only), ref_nparts entries
 //   win    : row window of a row-strip shard (null: the whole field; c.ny is
 //            then the buffer's rows and win->gny the field's)
+//   parts_cap: per-CTA partial records ws->parts can hold; a reducing launch
+//            uses at most parts_cap / K CTAs (and at most MAX_CTAS)
 // Returns a CUDA error code.
 struct RowWindow { int row0, gny, lo, hi; };
 cudaError_t launch_advance(int K, const double* Tin, double* Tout, const Coef& c,
                            const LaserSub* las, Partial* ring, Workspace* ws,
                            Partial* ref_out, long long ref_nparts, int rows,
-                           cudaStream_t stream, const RowWindow* win = nullptr);
+                           cudaStream_t stream, const RowWindow* win = nullptr,
+                           int parts_cap = MAX_CTAS * KMAX);
 
 // Extended-physics (phys == 1) single step, one thread per cell, with the
 // same reduction outputs as launch_advance.

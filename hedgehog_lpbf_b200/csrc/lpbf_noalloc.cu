@@ -29,12 +29,12 @@ namespace {
 
 // Most per-CTA partial records the scratch holds (grid size x steps per
 // launch): 4096 records = 98,560 bytes with the 256-byte counter header.
+// The launch path sizes the grid from the occupancy query and then clamps it
+// to NOALLOC_PARTIALS / depth CTAs (>= 1024 for depth <= 4), so the records
+// of one launch always fit, on any GPU and for either load path.
 constexpr int NOALLOC_PARTIALS = 4096;
 constexpr size_t NOALLOC_BYTES = 256 + size_t(NOALLOC_PARTIALS) * sizeof(Partial);
 static_assert(NOALLOC_BYTES == LPBF_B200_NOALLOC_SCRATCH_BYTES, "header constant");
-// The step kernel never has more than 4 CTAs resident per SM (its register
-// use, and >= 48 KB of shared memory per CTA on the TMA path, cap it there).
-constexpr int MAX_CTAS_PER_SM = 4;
 
 // Same layout as Workspace's header followed by NOALLOC_PARTIALS partials.
 // Held by every GPU that loads the library, for the life of the process.
@@ -66,12 +66,14 @@ using namespace lpbf_b200;
 extern "C" int lpbf_b200_advance_noalloc(double* T_a, double* T_b, const StepConst* k,
                                          const lpbf_tick* plan, int n_steps,
                                          const lpbf_b200_opts* opts, Partial* ring,
-                                         cudaStream_t stream, int* result_in_b) {
+                                         cudaStream_t stream, int* result_in_b,
+                                         unsigned int* err) {
     if (!k || k->nx < 2 || k->ny < 1 || (long long)k->nx * k->ny >= (1ll << 40) || !opts ||
         !T_a || !T_b || T_a == T_b || n_steps < 0 || (n_steps > 0 && !plan) || !result_in_b)
         return LPBF_ERR_ARG;
     if (opts->bc != 0 && opts->bc != 1) return LPBF_ERR_ARG;
-    if (opts->phys != 0) return LPBF_ERR_UNSUPPORTED;     // baseline physics only
+    if (opts->phys != 0 && opts->phys != 1) return LPBF_ERR_ARG;
+    if (opts->phys == 1) return LPBF_ERR_UNSUPPORTED;     // baseline physics only
     const size_t N = (size_t)k->nx * k->ny;
     if (T_a < T_b + N && T_b < T_a + N) return LPBF_ERR_ARG;
 
@@ -81,9 +83,6 @@ extern "C" int lpbf_b200_advance_noalloc(double* T_a, double* T_b, const StepCon
         depth = (n >= (1ll << 22)) ? 3 : (n >= (1ll << 18)) ? 2 : 1;
     }
     depth = std::min(std::max(depth, 1), 4);
-    // Reject configurations whose per-CTA partials would not fit the scratch.
-    if ((long long)sm_count() * MAX_CTAS_PER_SM * depth > NOALLOC_PARTIALS)
-        return LPBF_ERR_WORKSPACE;
 
     void* scratch = nullptr;
     const int st = scratch_address(&scratch);
@@ -101,12 +100,20 @@ extern "C" int lpbf_b200_advance_noalloc(double* T_a, double* T_b, const StepCon
         LaserSub las[KMAX];
         for (int t = 0; t < kk; ++t)
             las[t] = make_laser(*k, plan[s0 + t].x_l, plan[s0 + t].y_l, plan[s0 + t].q_scale);
-        if (launch_advance(kk, cur, nxt, c, las, ring ? ring + s0 : nullptr, ws, nullptr, 0,
-                           opts->rows, stream) != cudaSuccess)
-            return LPBF_ERR_CUDA;
+        const cudaError_t e = launch_advance(kk, cur, nxt, c, las, ring ? ring + s0 : nullptr,
+                                             ws, nullptr, 0, opts->rows, stream, nullptr,
+                                             NOALLOC_PARTIALS);
+        // a launch needing more per-CTA records than the scratch holds
+        if (e == cudaErrorInvalidValue) return LPBF_ERR_WORKSPACE;
+        if (e != cudaSuccess) return LPBF_ERR_CUDA;
         std::swap(cur, nxt);
         in_b ^= 1;
     }
+    // The error word lives in the shared scratch, which the caller cannot
+    // address: copy it out behind this call's launches.
+    if (err && cudaMemcpyAsync(err, &ws->err, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                               stream) != cudaSuccess)
+        return LPBF_ERR_CUDA;
     *result_in_b = in_b;
     return LPBF_OK;
 }

@@ -155,15 +155,24 @@ int lpbf_b200_f32k_join(const float* hi, const float* lo, double* T, size_t n,
  *    stream capture.
  *  - Every call clears and reuses the same array: calls that overlap on the
  *    GPU (other streams, other threads) race and must not be issued.
- *  - Baseline physics only (phys == 1 returns LPBF_ERR_UNSUPPORTED); a GPU
- *    needing more than 4096 per-CTA partial records for the requested depth
- *    is rejected with LPBF_ERR_WORKSPACE.
- * Inputs, outputs and results are as for lpbf_b200_advance. */
+ *  - Baseline physics only (phys == 1 returns LPBF_ERR_UNSUPPORTED, other
+ *    phys values LPBF_ERR_ARG, as lpbf_b200_advance).
+ *  - The array holds 4096 per-CTA partial records.  Each launch is clamped
+ *    to 4096 / depth CTAs, so every field size fits; a launch that would
+ *    still need more records is rejected with LPBF_ERR_WORKSPACE.
+ *  - err (host, nullable) receives the call's error word, which otherwise
+ *    stays inside the shared array: bit 0 = a bounded wait for a row copy
+ *    ran out and the field is incomplete, bit 1 = a NaN or infinite
+ *    temperature was seen by the per-step reduction (needs ring).  It is
+ *    copied behind the call's launches on `stream`: read it after the
+ *    stream has been synchronized.
+ * Inputs, outputs and results are otherwise as for lpbf_b200_advance. */
 #define LPBF_B200_NOALLOC_SCRATCH_BYTES 98560
 int lpbf_b200_advance_noalloc(double* T_a, double* T_b, const StepConst* k,
                               const lpbf_tick* plan, int n_steps,
                               const lpbf_b200_opts* opts, Partial* ring,
-                              cudaStream_t stream, int* result_in_b);
+                              cudaStream_t stream, int* result_in_b,
+                              unsigned int* err);
 
 /* ---- Batched process map ---------------------------------------------------
  * Replaces the reference's serial ensemble loop, one GpuStepTask graph per

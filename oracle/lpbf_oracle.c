@@ -63,6 +63,36 @@ double oracle_cp_eff(double T) {
     return c;
 }
 
+/* ---- one baseline cell (step_task.hpp:87-131; cpu_step baseline) ------ */
+static inline double base_cell(const double* Tin, const OracleStepConst* k, int x, int y,
+                               size_t c) {
+    const int nx = k->nx, ny = k->ny;
+    const double T = Tin[c];
+    const double xpos = (double)x * k->dx;
+    const double ypos = (double)y * k->dy;
+    const double r2 = (xpos - k->x_l) * (xpos - k->x_l)
+                    + (ypos - k->y_l) * (ypos - k->y_l);
+    double lap_x;
+    if (x == 0)           lap_x = (Tin[c + 1] - T) * k->inv_dx2;
+    else if (x == nx - 1) lap_x = (Tin[c - 1] - T) * k->inv_dx2;
+    else lap_x = (Tin[c + 1] - 2.0 * T + Tin[c - 1]) * k->inv_dx2;
+    const double Tym = (y == 0) ? T : Tin[c - nx];
+    const double Typ = (y == ny - 1) ? T : Tin[c + nx];
+    const double lap_y = (Typ - 2.0 * T + Tym) * k->inv_dy2;
+    const double S = k->q_scale * k->peak_S
+                   * exp(-2.0 * r2 * k->inv_r0_sq) / (k->rho_cp * k->h);
+    double q_top = k->hConv * (T - k->Tamb);
+    if (k->radiation) {
+        const double T4 = T * T * T * T;
+        const double Ta4 = k->Tamb * k->Tamb * k->Tamb * k->Tamb;
+        q_top += k->eps * SIGMA_SB * (T4 - Ta4);
+    }
+    const double q_bot = (k->K / k->dSub) * (T - k->Tsub);
+    const double loss = (q_top + q_bot) * k->inv_h / k->rho_cp;
+    const double dTdt = k->alpha * (lap_x + lap_y) + S - loss;
+    return T + k->dt * dTdt;
+}
+
 /* ---- one explicit-Euler step over the whole grid ---------------------- */
 void oracle_step(const double* Tin, double* Tout, const OracleStepConst* k,
                  int phys, int bc, double T_D) {
@@ -75,31 +105,13 @@ void oracle_step(const double* Tin, double* Tout, const OracleStepConst* k,
                 Tout[c] = T_D;
                 continue;
             }
-            const double T = Tin[c];
-            const double xpos = (double)x * k->dx;
-            const double r2 = (xpos - k->x_l) * (xpos - k->x_l)
-                            + (ypos - k->y_l) * (ypos - k->y_l);
             if (phys == 0) {
-                double lap_x;
-                if (x == 0)           lap_x = (Tin[c + 1] - T) * k->inv_dx2;
-                else if (x == nx - 1) lap_x = (Tin[c - 1] - T) * k->inv_dx2;
-                else lap_x = (Tin[c + 1] - 2.0 * T + Tin[c - 1]) * k->inv_dx2;
-                const double Tym = (y == 0) ? T : Tin[c - nx];
-                const double Typ = (y == ny - 1) ? T : Tin[c + nx];
-                const double lap_y = (Typ - 2.0 * T + Tym) * k->inv_dy2;
-                const double S = k->q_scale * k->peak_S
-                               * exp(-2.0 * r2 * k->inv_r0_sq) / (k->rho_cp * k->h);
-                double q_top = k->hConv * (T - k->Tamb);
-                if (k->radiation) {
-                    const double T4 = T * T * T * T;
-                    const double Ta4 = k->Tamb * k->Tamb * k->Tamb * k->Tamb;
-                    q_top += k->eps * SIGMA_SB * (T4 - Ta4);
-                }
-                const double q_bot = (k->K / k->dSub) * (T - k->Tsub);
-                const double loss = (q_top + q_bot) * k->inv_h / k->rho_cp;
-                const double dTdt = k->alpha * (lap_x + lap_y) + S - loss;
-                Tout[c] = T + k->dt * dTdt;
+                Tout[c] = base_cell(Tin, k, x, y, c);
             } else {
+                const double T = Tin[c];
+                const double xpos = (double)x * k->dx;
+                const double r2 = (xpos - k->x_l) * (xpos - k->x_l)
+                                + (ypos - k->y_l) * (ypos - k->y_l);
                 const double Txm = (x == 0) ? T : Tin[c - 1];
                 const double Txp = (x == nx - 1) ? T : Tin[c + 1];
                 const double Tym = (y == 0) ? T : Tin[c - nx];
@@ -220,4 +232,269 @@ int oracle_run(double* T_a, double* T_b, const OracleStepConst* k0,
         if (ring) oracle_reduce(cur, k.nx, k.ny, Tm, &ring[s]);
     }
     return which;   /* 0: result in T_a, 1: result in T_b */
+}
+
+/* ---- n steps, computed only where the field can change -----------------
+ * The same steps as oracle_run (baseline physics), for fields that sit at a
+ * quiet temperature Q = Tamb = Tsub away from the laser's track (uniform
+ * starts, as in every workload of the benchmark).  In the reference's
+ * arithmetic a cell at Q whose four neighbours are at Q has a Laplacian of
+ * exactly 0 ((Q - 2Q) + Q and Q - Q are exact) and a loss of exactly 0
+ * (T - Tamb, T^4 - Ta^4 and T - Tsub are computed from equal operands), so
+ * its new value is Q + dt*S, which rounds back to Q wherever dt*S is below
+ * a quarter of an ulp of Q.  Such cells are not computed but set to Q, so
+ * the result is bit-identical to oracle_run's (tests/test_oracle.py checks
+ * the two against each other).  Per step, the cells computed are the
+ * bounding box of the input's non-Q cells grown by one cell, joined with
+ * the box outside of which the laser's dt*S is provably below that bound.
+ * Rows of that box are shared among n_threads POSIX threads (each cell is
+ * computed independently, so the thread count changes no result); the
+ * per-step Partial is combined serially in flat-index order, as in
+ * oracle_reduce.  Fixed edges (bc 1) are allowed when T_D == Q.
+ * Returns which buffer holds the result (0: T_a, 1: T_b), or -1 when the
+ * preconditions fail (the caller then uses oracle_run).  T_b is scratch.
+ * probe_idx/probe_val (nullable): probe_val[s] = the field after step s at
+ * flat index probe_idx[s].
+ */
+#include <pthread.h>
+#include <stdlib.h>
+
+typedef struct { int x0, x1, y0, y1; } QBox;   /* inclusive; empty if x0 > x1 */
+
+static QBox qbox_empty(void) { QBox b = {1, 0, 1, 0}; return b; }
+static int qbox_is_empty(QBox b) { return b.x0 > b.x1 || b.y0 > b.y1; }
+static QBox qbox_join(QBox a, QBox b) {
+    if (qbox_is_empty(a)) return b;
+    if (qbox_is_empty(b)) return a;
+    QBox r = {a.x0 < b.x0 ? a.x0 : b.x0, a.x1 > b.x1 ? a.x1 : b.x1,
+              a.y0 < b.y0 ? a.y0 : b.y0, a.y1 > b.y1 ? a.y1 : b.y1};
+    return r;
+}
+static QBox qbox_grow_clip(QBox b, int g, int nx, int ny) {
+    if (qbox_is_empty(b)) return b;
+    QBox r = {b.x0 - g, b.x1 + g, b.y0 - g, b.y1 + g};
+    if (r.x0 < 0) r.x0 = 0;
+    if (r.y0 < 0) r.y0 = 0;
+    if (r.x1 > nx - 1) r.x1 = nx - 1;
+    if (r.y1 > ny - 1) r.y1 = ny - 1;
+    return r;
+}
+static int qbox_has(QBox b, int x, int y) {
+    return x >= b.x0 && x <= b.x1 && y >= b.y0 && y <= b.y1;
+}
+
+/* Cells outside the returned box get dt*S <= ulp(Q)/8 from laser (x_l, y_l,
+ * q); a whole-field box when the laser values are not finite. */
+static QBox laser_box(const OracleStepConst* k, double Q) {
+    const int nx = k->nx, ny = k->ny;
+    QBox all = {0, nx - 1, 0, ny - 1};
+    if (!isfinite(k->x_l) || !isfinite(k->y_l) || !isfinite(k->q_scale)) return all;
+    if (k->q_scale == 0.0) return qbox_empty();            /* S = 0 * ... = 0 */
+    const double amp = fabs(k->dt * k->q_scale * k->peak_S / (k->rho_cp * k->h));
+    const double u = (nextafter(Q, INFINITY) - Q) / 8.0;
+    if (!isfinite(amp)) return all;
+    if (amp <= u) return qbox_empty();                     /* exp <= 1 */
+    /* exp(-2 r^2 / r0^2) <= u / amp  <=>  r^2 >= ln(amp / u) r0^2 / 2; two
+     * more units in the exponent (a factor e^-2) cover the roundings */
+    const double r2 = (log(amp / u) + 2.0) / (2.0 * k->inv_r0_sq);
+    const double R = sqrt(r2);
+    if (!isfinite(R) || k->dx <= 0.0 || k->dy <= 0.0) return all;
+    double fx0 = floor((k->x_l - R) / k->dx) - 1.0, fx1 = ceil((k->x_l + R) / k->dx) + 1.0;
+    double fy0 = floor((k->y_l - R) / k->dy) - 1.0, fy1 = ceil((k->y_l + R) / k->dy) + 1.0;
+    if (fx1 < 0.0 || fy1 < 0.0 || fx0 > nx - 1.0 || fy0 > ny - 1.0) return qbox_empty();
+    QBox b = {fx0 < 0.0 ? 0 : (int)fx0, fx1 > nx - 1.0 ? nx - 1 : (int)fx1,
+              fy0 < 0.0 ? 0 : (int)fy0, fy1 > ny - 1.0 ? ny - 1 : (int)fy1};
+    return b;
+}
+
+typedef struct {
+    /* set by the coordinating thread before each step */
+    const double* in;
+    double* out;
+    OracleStepConst k;
+    QBox C;
+    int bc;
+    double T_D, Tm, Q;
+    /* per-row results of the step */
+    double* row_tmax;
+    long long* row_arg;
+    int* row_xlo;
+    int* row_xhi;
+    char* row_hot;
+    /* row claiming and step barriers */
+    volatile int next_row;
+    int done;
+    pthread_barrier_t bar;
+} QShared;
+
+static void quiet_rows(QShared* sh) {
+    const OracleStepConst* k = &sh->k;
+    const int nx = k->nx, ny = k->ny;
+    const long long N = (long long)nx * ny;
+    const QBox C = sh->C;
+    const int nrows = C.y1 - C.y0 + 1;
+    for (;;) {
+        const int r = __sync_fetch_and_add(&sh->next_row, 1);
+        if (r >= nrows) break;
+        const int y = C.y0 + r;
+        double tmax = -1.0;
+        long long arg = N;
+        int xlo = nx, xhi = -1;
+        char hot = 0;
+        for (int x = C.x0; x <= C.x1; ++x) {
+            const size_t c = (size_t)y * nx + x;
+            double v;
+            if (sh->bc == 1 && (x == 0 || y == 0 || x == nx - 1 || y == ny - 1))
+                v = sh->T_D;
+            else
+                v = base_cell(sh->in, k, x, y, c);
+            sh->out[c] = v;
+            if (v > tmax) { tmax = v; arg = (long long)c; }
+            if (v > sh->Tm) hot = 1;
+            if (v != sh->Q) { if (x < xlo) xlo = x; xhi = x; }
+        }
+        sh->row_tmax[y] = tmax;
+        sh->row_arg[y] = arg;
+        sh->row_xlo[y] = xlo;
+        sh->row_xhi[y] = xhi;
+        sh->row_hot[y] = hot;
+    }
+}
+
+static void* quiet_worker(void* arg) {
+    QShared* sh = (QShared*)arg;
+    for (;;) {
+        pthread_barrier_wait(&sh->bar);          /* step set up (or done) */
+        if (sh->done) break;
+        quiet_rows(sh);
+        pthread_barrier_wait(&sh->bar);          /* step's rows finished */
+    }
+    return NULL;
+}
+
+/* Smallest flat index outside box C (N when C covers the field). */
+static long long first_outside(QBox C, int nx, int ny) {
+    if (qbox_is_empty(C) || C.y0 > 0 || C.x0 > 0) return 0;
+    if (C.x1 < nx - 1) return C.x1 + 1;
+    if (C.y1 < ny - 1) return (long long)(C.y1 + 1) * nx;
+    return (long long)nx * ny;
+}
+
+int oracle_run_quiet(double* T_a, double* T_b, const OracleStepConst* k0,
+                     const OracleLaser* plan, int n_steps, int bc, double T_D, double Tm,
+                     OraclePartial* ring, int n_threads, const long long* probe_idx,
+                     double* probe_val) {
+    const int nx = k0->nx, ny = k0->ny;
+    const double Q = k0->Tamb;
+    if (nx < 2 || ny < 2 || k0->Tsub != Q || !isfinite(Q) || Tm < Q ||
+        (bc != 0 && bc != 1) || (bc == 1 && T_D != Q))
+        return -1;
+    /* the zero Laplacian and loss at Q need finite coefficients */
+    const double coef[] = {k0->alpha, k0->inv_dx2, k0->inv_dy2, k0->hConv, k0->eps,
+                           k0->K / k0->dSub, k0->inv_h, k0->rho_cp, k0->dt};
+    for (size_t i = 0; i < sizeof(coef) / sizeof(coef[0]); ++i)
+        if (!isfinite(coef[i])) return -1;
+    const long long N = (long long)nx * ny;
+    if (n_threads < 1) n_threads = 1;
+    if (n_threads > 256) n_threads = 256;
+
+    QShared sh;
+    memset(&sh, 0, sizeof(sh));
+    sh.k = *k0;
+    sh.bc = bc; sh.T_D = T_D; sh.Tm = Tm; sh.Q = Q;
+    sh.row_tmax = (double*)malloc(sizeof(double) * ny);
+    sh.row_arg = (long long*)malloc(sizeof(long long) * ny);
+    sh.row_xlo = (int*)malloc(sizeof(int) * ny);
+    sh.row_xhi = (int*)malloc(sizeof(int) * ny);
+    sh.row_hot = (char*)malloc(ny);
+    pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * n_threads);
+    if (!sh.row_tmax || !sh.row_arg || !sh.row_xlo || !sh.row_xhi || !sh.row_hot || !th) {
+        free(sh.row_tmax); free(sh.row_arg); free(sh.row_xlo); free(sh.row_xhi);
+        free(sh.row_hot); free(th);
+        return -1;
+    }
+
+    /* non-Q box of the start field; the scratch buffer starts all Q */
+    QBox A = qbox_empty();
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) {
+            const double v = T_a[(size_t)y * nx + x];
+            if (v != Q) {
+                QBox one = {x, x, y, y};
+                A = qbox_join(A, one);
+            }
+        }
+    for (long long i = 0; i < N; ++i) T_b[i] = Q;
+    QBox dirty[2] = {A, qbox_empty()};   /* cells of each buffer that may differ from Q */
+
+    pthread_barrier_init(&sh.bar, NULL, (unsigned)n_threads);
+    for (int t = 1; t < n_threads; ++t) pthread_create(&th[t], NULL, quiet_worker, &sh);
+
+    double* buf[2] = {T_a, T_b};
+    int cur = 0;
+    for (int s = 0; s < n_steps; ++s) {
+        sh.k.x_l = plan[s].x_l;
+        sh.k.y_l = plan[s].y_l;
+        sh.k.q_scale = plan[s].q_scale;
+        const QBox C = qbox_join(qbox_grow_clip(A, 1, nx, ny), laser_box(&sh.k, Q));
+        const int nxt = cur ^ 1;
+        sh.in = buf[cur];
+        sh.out = buf[nxt];
+        sh.C = C;
+        sh.next_row = 0;
+        if (!qbox_is_empty(C)) {
+            pthread_barrier_wait(&sh.bar);
+            quiet_rows(&sh);
+            pthread_barrier_wait(&sh.bar);
+        }
+        /* cells of the output buffer outside C return to Q */
+        const QBox D = dirty[nxt];
+        if (!qbox_is_empty(D))
+            for (int y = D.y0; y <= D.y1; ++y)
+                for (int x = D.x0; x <= D.x1; ++x)
+                    if (!qbox_has(C, x, y)) buf[nxt][(size_t)y * nx + x] = Q;
+        dirty[nxt] = C;
+
+        /* non-Q box and the step's Partial, rows in ascending order */
+        A = qbox_empty();
+        double tin = -1.0;
+        long long ain = N;
+        int ymin = ny, ymax = -1;
+        if (!qbox_is_empty(C))
+            for (int y = C.y0; y <= C.y1; ++y) {
+                if (sh.row_xlo[y] <= sh.row_xhi[y]) {
+                    QBox rb = {sh.row_xlo[y], sh.row_xhi[y], y, y};
+                    A = qbox_join(A, rb);
+                }
+                if (sh.row_tmax[y] > tin) { tin = sh.row_tmax[y]; ain = sh.row_arg[y]; }
+                if (sh.row_hot[y]) { if (y < ymin) ymin = y; ymax = y; }
+            }
+        if (ring) {
+            /* every cell outside C holds Q (Q <= Tm: never molten) */
+            const long long fo = first_outside(C, nx, ny);
+            double tout = -1.0;
+            long long aout = N;
+            if (fo < N && Q > -1.0) { tout = Q; aout = fo; }
+            OraclePartial p;
+            if (tout > tin) { p.tmax = tout; p.arg = aout; }
+            else if (tin > tout) { p.tmax = tin; p.arg = ain; }
+            else { p.tmax = tin; p.arg = ain < aout ? ain : aout; }
+            p.ymin = ymin;
+            p.ymax = ymax;
+            ring[s] = p;
+        }
+        /* the value after step s at a cell named by the caller (a checker
+         * asks for the cell another implementation reported as the peak) */
+        if (probe_idx && probe_val)
+            probe_val[s] = (probe_idx[s] >= 0 && probe_idx[s] < N)
+                               ? buf[nxt][probe_idx[s]] : NAN;
+        cur = nxt;
+    }
+    sh.done = 1;
+    pthread_barrier_wait(&sh.bar);
+    for (int t = 1; t < n_threads; ++t) pthread_join(th[t], NULL);
+    pthread_barrier_destroy(&sh.bar);
+    free(sh.row_tmax); free(sh.row_arg); free(sh.row_xlo); free(sh.row_xhi);
+    free(sh.row_hot); free(th);
+    return cur;
 }

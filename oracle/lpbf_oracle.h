@@ -38,6 +38,10 @@ double oracle_w_sub(const double* col, int ny, double dy, double Tm);
 int oracle_run(double* T_a, double* T_b, const OracleStepConst* k0,
                const OracleLaser* plan, int n_steps, int phys, int bc,
                double T_D, double Tm, OraclePartial* ring);
+int oracle_run_quiet(double* T_a, double* T_b, const OracleStepConst* k0,
+                     const OracleLaser* plan, int n_steps, int bc, double T_D, double Tm,
+                     OraclePartial* ring, int n_threads, const long long* probe_idx,
+                     double* probe_val);
 
 #ifdef __cplusplus
 }

@@ -89,6 +89,10 @@ def lib():
                                      ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_void_p]
             L.oracle_run.restype = ctypes.c_int
+            L.oracle_run_quiet.argtypes = [_dp, _dp, sc, _dp, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                           ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+            L.oracle_run_quiet.restype = ctypes.c_int
             for f in ("oracle_k_of", "oracle_cp_of", "oracle_cp_eff"):
                 getattr(L, f).argtypes = [ctypes.c_double]
                 getattr(L, f).restype = ctypes.c_double
@@ -147,7 +151,55 @@ def run(T0: np.ndarray, k, laser: np.ndarray, phys: int = 0, bc: int = 0,
     return (b if which else a), ring
 
 
+def run_quiet(T0: np.ndarray, k, laser: np.ndarray, bc: int = 0, T_D: float = 300.0,
+              Tm: float = 1609.0, with_ring: bool = True, threads: int | None = None,
+              probe: np.ndarray | None = None):
+    """``run`` for the baseline physics, computing per step only the cells
+    that can differ from the quiet temperature Tamb (= Tsub) and sharing
+    them among threads: bit-identical results, far less work on large
+    fields heated along a track.  Raises when its preconditions (Tamb ==
+    Tsub, fixed edges at Tamb, Tm >= Tamb) do not hold.
+
+    probe (optional, one flat index per step): also returns the field's
+    value at probe[s] after step s, as a third result."""
+    a = np.array(T0, dtype=np.float64, copy=True, order="C")
+    b = np.empty_like(a)
+    laser = np.ascontiguousarray(laser, dtype=np.float64)
+    n = laser.shape[0]
+    ring = np.zeros(n, dtype=PARTIAL_DTYPE) if with_ring else None
+    kk = as_const(k)
+    nt = threads or min(64, os.cpu_count() or 1)
+    pidx = pval = None
+    if probe is not None:
+        pidx = np.ascontiguousarray(probe, dtype=np.int64)
+        assert pidx.shape == (n,)
+        pval = np.full(n, np.nan)
+    which = lib().oracle_run_quiet(_ptr(a), _ptr(b), ctypes.byref(kk), _ptr(laser), n, bc, T_D,
+                                   Tm, ring.ctypes.data if ring is not None else None, nt,
+                                   pidx.ctypes.data if pidx is not None else None,
+                                   pval.ctypes.data if pval is not None else None)
+    if which < 0:
+        raise ValueError("run_quiet needs Tamb == Tsub, fixed edges at Tamb and Tm >= Tamb")
+    T = b if which else a
+    return (T, ring, pval) if probe is not None else (T, ring)
+
+
 # ---- the reference's own code (oracle/_ref) --------------------------------
+
+def reference_tree() -> str | None:
+    """The reference source tree: $LPBF_REFERENCE, else the location the last
+    ``make -C oracle ref`` run by the build recorded in oracle/_ref, else
+    None (no default path)."""
+    env = os.environ.get("LPBF_REFERENCE")
+    if env:
+        return env
+    rec = os.path.join(_REF, "REFERENCE_TREE")
+    if os.path.exists(rec):
+        with open(rec) as f:
+            p = f.read().strip()
+        return p or None
+    return None
+
 
 def have_reference() -> bool:
     return all(os.path.exists(os.path.join(_REF, f))
@@ -192,6 +244,12 @@ def ref_lib(name: str = "libref.so"):
                                              ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_void_p]
                 L.ref_build_plan.restype = ctypes.c_int
+                L.ref_gpu_task_run.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                               ctypes.c_double, ctypes.POINTER(OracleStepConst),
+                                               ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]
+                L.ref_gpu_task_run.restype = ctypes.c_double
             _ref[name] = L
     return _ref[name]
 
@@ -244,6 +302,21 @@ def ref_run_cpu(mat, pr, dom, dt, n_steps, phys=0, kmult=1.0):
                                  ctypes.byref(pk), ctypes.byref(pw), ctypes.byref(ws))
     return dict(T=T.reshape(dom.ny, dom.nx), peak_T=pk.value, peak_W=pw.value,
                 steady_W_sub=ws.value, wall_ms=wall)
+
+
+def ref_gpu_task_run(k, dom, plan: np.ndarray, Tm: float, Tamb: float, batch: int = 64,
+                     mode: int = 2, fused: bool = False, pinned: bool = False):
+    """The reference's own GpuStepTask graph (its kernels, built for sm_100a)
+    over ``plan`` (Tick array) on the current CUDA device.  Returns (wall ms
+    from the first Tick to the graph's end, the run's peak temperature)."""
+    plan = np.ascontiguousarray(plan)
+    assert plan.dtype.itemsize == 56
+    kk = as_const(k)
+    pk = ctypes.c_double()
+    ms = ref_lib("libref_plan.so").ref_gpu_task_run(
+        dom.nx, dom.ny, dom.Lx, dom.Ly, ctypes.byref(kk), Tm, Tamb, plan.ctypes.data,
+        len(plan), batch, mode, int(fused), int(pinned), ctypes.byref(pk))
+    return ms, pk.value
 
 
 def ref_build_plan(pr, dom, dt, n_steps, snap_every, tick_dtype) -> np.ndarray:

@@ -1,8 +1,9 @@
 # SPDX-License-Identifier: 0BSD
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a checkout where the reference tree is available (default
-/root/reference, override with LPBF_REFERENCE) after ``make -C oracle ref``:
+Run in a checkout where the reference tree is available (LPBF_REFERENCE, or
+the location recorded by ``make -C oracle ref`` through the build) after
+building oracle/_ref:
 
     python tests/golden/make_golden.py
 
@@ -32,7 +33,9 @@ from hedgehog_lpbf_b200 import params as P  # noqa: E402
 from hedgehog_lpbf_b200 import plan as PL  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-REF = os.environ.get("LPBF_REFERENCE", "/root/reference")
+REF = O.reference_tree()
+if not REF:
+    sys.exit("make_golden.py: set LPBF_REFERENCE to the reference source tree")
 
 
 def case0():

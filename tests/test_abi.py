@@ -75,8 +75,9 @@ def test_gpu_step_task_header_builds_against_library():
     d = os.path.join(ROOT, "tests", "dropin")
     subprocess.run(["make", "-s", "-C", d, "demo"], check=True)
     assert os.path.exists(os.path.join(ROOT, "tests", "_build", "gpu_task_demo"))
-    ref = os.environ.get("LPBF_REFERENCE", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "src", "gpu")):
+    from oracle import oracle as O
+    ref = O.reference_tree()
+    if ref and os.path.isdir(os.path.join(ref, "src", "gpu")):
         subprocess.run(["make", "-s", "-C", d, "ref", f"REF={ref}"], check=True)
         assert os.path.exists(os.path.join(ROOT, "tests", "_build", "ref_hhcuda_on_b200"))
 

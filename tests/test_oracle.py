@@ -184,3 +184,41 @@ def test_reference_cpu_step_matches_oracle_random_cases(seed):
     T_o, _ = O.run(T0, k, las, with_ring=False)
     T_r = O.ref_run_plan(T0, k, las)
     assert np.array_equal(T_o, T_r)
+
+
+@pytest.mark.parametrize("case", ["uniform_raster", "warm_patch_fixed_edges", "edge_corner",
+                                  "nan_and_ties"])
+def test_quiet_run_bit_identical_to_full_run(case):
+    """oracle.run_quiet (cells that provably stay at Tamb skipped, rows shared
+    among threads) equals the full-grid oracle.run bit for bit, field and
+    every per-step Partial, whatever the thread count; its probe reads the
+    field after each step."""
+    mat, pr = P.benchmark_material_process()
+    nx, ny, n, bc = 300, 220, 240, 0
+    dom = P.Domain(Lx=(nx - 1) * 5e-6, Ly=(ny - 1) * 5e-6, nx=nx, ny=ny)
+    k = P.make_const(mat, pr, dom, P.dt_fraction(mat, dom))
+    T0 = np.full(nx * ny, 300.0)
+    plan = PL.raster_for_steps(dom, k.dt, n, V=1.0, hatch=100e-6, n_tracks=3, angle=0.3)
+    if case == "warm_patch_fixed_edges":
+        bc = 1
+        rng = np.random.default_rng(4)
+        T0.reshape(ny, nx)[40:90, 200:260] = 300.0 + rng.uniform(0.0, 900.0, (50, 60))
+    elif case == "edge_corner":
+        plan = PL.raster(dom, k.dt, n, V=1.0, hatch=100e-6, track_len=0.6e-3, n_tracks=3,
+                         center=(0.05e-3, 0.08e-3))
+    elif case == "nan_and_ties":
+        T0.reshape(ny, nx)[100, 50] = np.nan
+        T0.reshape(ny, nx)[[10, 30], [20, 20]] = 5000.0   # two equal peaks
+        plan["q_scale"][::3] = 0.0
+    las = PL.laser_array(plan)
+    T_ref, ring_ref = O.run(T0, k, las, bc=bc, Tm=mat.Tm)
+    probe = np.arange(n, dtype=np.int64) * 211 % (nx * ny)
+    for threads in (1, 4):
+        T, ring, pv = O.run_quiet(T0, k, las, bc=bc, Tm=mat.Tm, threads=threads, probe=probe)
+        assert np.array_equal(T.view(np.uint64), T_ref.view(np.uint64)), threads
+        assert ring.tobytes() == ring_ref.tobytes(), threads
+    assert np.array_equal(pv[-1:], T_ref[probe[-1:]], equal_nan=True)
+    with pytest.raises(ValueError):
+        k2 = P.make_const(mat, pr, dom, k.dt)
+        k2.Tsub = 420.0
+        O.run_quiet(T0, k2, las[:2], Tm=mat.Tm)

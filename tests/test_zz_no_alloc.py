@@ -7,9 +7,10 @@ device pointers through, hosts where a cudaMalloc would synchronize the
 device at a forbidden point): it takes no workspace and keeps its scratch in
 a fixed array inside the library.  This file checks, through the C-ABI, that
 two calls in a row give the same fields and per-step Partials as the
-workspace entry point, lpbf_b200_advance, within the parity tolerance used
-throughout (max relative error 1e-12 on the field, exact Partials), and that
-it rejects what it does not support.  It is named to be collected last.
+workspace entry point, lpbf_b200_advance, on both load paths (TMA-fed rows
+for even widths, direct loads for odd ones) and every depth, that the error
+word the caller cannot otherwise reach is handed back, and that it rejects
+what it does not support.  It is named to be collected last.
 """
 import ctypes
 
@@ -34,11 +35,13 @@ def _advance(L, torch, k, plan, T0, opts, noalloc, work=None):
     n = len(plan)
     ring = torch.zeros(24 * n, dtype=torch.uint8, device=dev)
     in_b = ctypes.c_int(-1)
+    err = ctypes.c_uint(0xFFFFFFFF)
     stream = torch.cuda.current_stream().cuda_stream
     if noalloc:
         st = L.lpbf_b200_advance_noalloc(a.data_ptr(), b.data_ptr(), ctypes.byref(k),
                                          plan.ctypes.data, n, ctypes.byref(opts),
-                                         ring.data_ptr(), stream, ctypes.byref(in_b))
+                                         ring.data_ptr(), stream, ctypes.byref(in_b),
+                                         ctypes.byref(err))
     else:
         st = L.lpbf_b200_advance(a.data_ptr(), b.data_ptr(), ctypes.byref(k), plan.ctypes.data,
                                  n, ctypes.byref(opts), ring.data_ptr(), work.data_ptr(),
@@ -46,47 +49,79 @@ def _advance(L, torch, k, plan, T0, opts, noalloc, work=None):
     assert st == 0, L.lpbf_b200_status_string(st)
     torch.cuda.synchronize()
     T = (b if in_b.value else a).cpu().numpy()
-    return T, ring.cpu().numpy()
+    return T, ring.cpu().numpy(), err.value
 
 
-@pytest.mark.parametrize("depth", [3, 4])
-def test_no_alloc_matches_workspace_entry_point_twice(gpu, depth):
-    import torch
-    from hedgehog_lpbf_b200 import _lib
-    L = _lib.lib()
+def _setup(L, torch, nx, ny):
     mat, pr = P.benchmark_material_process()
-    dom = P.Domain(Lx=511 * 5e-6, Ly=383 * 5e-6, nx=512, ny=384)
+    dom = P.Domain(Lx=(nx - 1) * 5e-6, Ly=(ny - 1) * 5e-6, nx=nx, ny=ny)
     k = P.make_const(mat, pr, dom, P.dt_fraction(mat, dom))
-    opts = _lib.Opts(phys=0, bc=0, T_edge=300.0, Tm=mat.Tm, depth=depth, rows=0)
     work = torch.empty(L.lpbf_b200_workspace_bytes(), dtype=torch.uint8, device="cuda:0")
     assert L.lpbf_b200_workspace_init(work.data_ptr(), work.numel(),
                                       torch.cuda.current_stream().cuda_stream) == 0
+    return mat, pr, dom, k, work
+
+
+# (512, 384): TMA-fed rows; (513, 384): odd width, the direct-load kernel
+@pytest.mark.parametrize("shape", [(512, 384), (513, 384)])
+@pytest.mark.parametrize("depth", [1, 2, 3, 4])
+def test_no_alloc_matches_workspace_entry_point_twice(gpu, shape, depth):
+    import torch
+    from hedgehog_lpbf_b200 import _lib
+    L = _lib.lib()
+    nx, ny = shape
+    mat, pr, dom, k, work = _setup(L, torch, nx, ny)
+    opts = _lib.Opts(phys=0, bc=0, T_edge=300.0, Tm=mat.Tm, depth=depth, rows=0)
     rng = np.random.default_rng(depth)
     cases = [
-        (np.full(512 * 384, 300.0), PL.single_track(pr, dom, k.dt, 37)),
-        (300.0 + rng.uniform(0.0, 2000.0, 512 * 384),
+        (np.full(nx * ny, 300.0), PL.single_track(pr, dom, k.dt, 37)),
+        (300.0 + rng.uniform(0.0, 2000.0, nx * ny),
          PL.raster_for_steps(dom, k.dt, 29, V=1.0, hatch=100e-6, n_tracks=2, angle=0.4)),
     ]
     for T0, plan in cases:                     # two calls in a row
-        T_ref, r_ref = _advance(L, torch, k, plan, T0, opts, noalloc=False, work=work)
-        T_na, r_na = _advance(L, torch, k, plan, T0, opts, noalloc=True)
+        T_ref, r_ref, _ = _advance(L, torch, k, plan, T0, opts, noalloc=False, work=work)
+        T_na, r_na, err = _advance(L, torch, k, plan, T0, opts, noalloc=True)
         assert _rel_err(T_na, T_ref) <= RTOL
+        # the same kernel on the same inputs: identical bits and Partials
+        assert np.array_equal(T_na.view(np.uint64), T_ref.view(np.uint64))
         assert r_na.tobytes() == r_ref.tobytes()
+        assert err == 0
 
 
-def test_no_alloc_rejects_extended_physics(gpu):
+def test_no_alloc_reports_non_finite_temperature(gpu):
+    """A NaN in the start field is reported through the error word (bit 1);
+    the next clean call starts from a cleared word."""
+    import torch
+    from hedgehog_lpbf_b200 import _lib
+    L = _lib.lib()
+    nx, ny = 256, 128
+    mat, pr, dom, k, work = _setup(L, torch, nx, ny)
+    opts = _lib.Opts(phys=0, bc=0, T_edge=300.0, Tm=mat.Tm, depth=3, rows=0)
+    plan = PL.single_track(pr, dom, k.dt, 6)
+    T0 = np.full(nx * ny, 300.0)
+    T0[ny // 2 * nx + 17] = np.nan
+    _, _, err = _advance(L, torch, k, plan, T0, opts, noalloc=True)
+    assert err & 2
+    _, _, err = _advance(L, torch, k, plan, np.full(nx * ny, 300.0), opts, noalloc=True)
+    assert err == 0
+
+
+def test_no_alloc_rejects_what_it_does_not_run(gpu):
     import torch
     from hedgehog_lpbf_b200 import _lib
     L = _lib.lib()
     mat, pr = P.benchmark_material_process()
     dom = P.square_domain(64)
     k = P.make_const(mat, pr, dom, P.dt_fraction(mat, dom))
-    opts = _lib.Opts(phys=1, bc=0, T_edge=300.0, Tm=mat.Tm, depth=1, rows=0)
     a = torch.full((64, 64), 300.0, dtype=torch.float64, device="cuda:0")
     b = torch.empty_like(a)
     plan = PL.single_track(pr, dom, k.dt, 2)
     in_b = ctypes.c_int(0)
-    st = L.lpbf_b200_advance_noalloc(a.data_ptr(), b.data_ptr(), ctypes.byref(k),
-                                     plan.ctypes.data, 2, ctypes.byref(opts), None,
-                                     torch.cuda.current_stream().cuda_stream, ctypes.byref(in_b))
-    assert st == -2
+    stream = torch.cuda.current_stream().cuda_stream
+    # extended physics: a valid request this entry point does not implement
+    for phys, want in ((1, -2), (2, -1), (-1, -1)):
+        opts = _lib.Opts(phys=phys, bc=0, T_edge=300.0, Tm=mat.Tm, depth=1, rows=0)
+        st = L.lpbf_b200_advance_noalloc(a.data_ptr(), b.data_ptr(), ctypes.byref(k),
+                                         plan.ctypes.data, 2, ctypes.byref(opts), None, stream,
+                                         ctypes.byref(in_b), None)
+        assert st == want, (phys, st)
