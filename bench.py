@@ -190,7 +190,25 @@ def cpu_single_thread_rate(mat, pr, dom, k, budget_s: float):
                       f"{dom.nx}x{dom.ny}"}
 
 
-def reference_gpu_rate(mat, pr, dom, k, plan, n1: int = 192, n2: int = 1216):
+def reference_gpu_rate(timeout_s: float = 600.0):
+    """reference_gpu_child() in a child process on the same GPU: the
+    reference's task aborts its process on a CUDA error, which must not end
+    the bench.  Returns its result, or a record of why there is none."""
+    import subprocess
+    try:
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-gpu-child",
+                            "--side", str(N_SIDE)], capture_output=True, text=True,
+                           timeout=timeout_s)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": f"reference GPU task graph exceeded {timeout_s:.0f} s"}
+    for ln in r.stdout.splitlines()[::-1]:
+        if ln.startswith("{"):
+            return json.loads(ln)
+    tail = (r.stderr or r.stdout).strip().splitlines()[-1:] or [""]
+    return {"unavailable": f"reference GPU task graph exited {r.returncode}: {tail[0][:200]}"}
+
+
+def reference_gpu_child(n1: int = 192, n2: int = 1216):
     """The reference's own GPU path on this GPU: its GpuStepTask graph
     (include/gpu_step_task.hpp, run as run_one_row does, hh_gpu_main.cpp:171-
     207) with its kernels (src/gpu/kernels.cu built for sm_100a), default
@@ -198,19 +216,22 @@ def reference_gpu_rate(mat, pr, dom, k, plan, n1: int = 192, n2: int = 1216):
     step+reduce kernel, over the bench's raster plan.  Steady-state rate from
     two run lengths (the task's device set-up cancels in the difference)."""
     from oracle import oracle as O
+    mat, pr, dom, k, plan = workload(0)
     if not O.have_reference():
-        return None
+        return {"unavailable": "oracle/_ref (the reference built from its sources) is absent"}
     out = {"unit": "GCell-updates/s", "kind": "reference",
            "what": "reference GpuStepTask graph (mode 2, batch 64) with its own kernels "
                    "(kernels.cu built for sm_100a), wall clock, "
                    f"({n2} - {n1}) steps of {dom.nx}x{dom.ny} on the bench's raster"}
-    for name, fused in (("unfused", False), ("fused", True)):
-        O.ref_gpu_task_run(k, dom, plan[:64], mat.Tm, pr.Tamb, fused=fused)     # warm-up
-        t1, _ = O.ref_gpu_task_run(k, dom, plan[:n1], mat.Tm, pr.Tamb, fused=fused)
-        t2, pk = O.ref_gpu_task_run(k, dom, plan[:n2], mat.Tm, pr.Tamb, fused=fused)
-        out[name] = {"value": dom.nx * dom.ny * (n2 - n1) / ((t2 - t1) * 1e-3) / 1e9,
-                     "ms_per_step": (t2 - t1) / (n2 - n1), "peak_T_K": pk}
+    with ClockSampler(0) as clk:
+        for name, fused in (("unfused", False), ("fused", True)):
+            O.ref_gpu_task_run(k, dom, plan[:64], mat.Tm, pr.Tamb, fused=fused)     # warm-up
+            t1, _ = O.ref_gpu_task_run(k, dom, plan[:n1], mat.Tm, pr.Tamb, fused=fused)
+            t2, pk = O.ref_gpu_task_run(k, dom, plan[:n2], mat.Tm, pr.Tamb, fused=fused)
+            out[name] = {"value": dom.nx * dom.ny * (n2 - n1) / ((t2 - t1) * 1e-3) / 1e9,
+                         "ms_per_step": (t2 - t1) / (n2 - n1), "peak_T_K": pk}
     out["value"] = max(out["unfused"]["value"], out["fused"]["value"])
+    out["clocks"] = clk.summary()
     return out
 
 
@@ -244,7 +265,7 @@ def run_reference_arm(args, rank, world):
         have_gpu = False
     if have_gpu and N_SIDE == 8192 and not args.no_ref_gpu:
         # beside the CPU figure: the reference's own GPU task graph on this GPU
-        line["ref_gpu"] = reference_gpu_rate(mat, pr, dom, k, plan)
+        line["ref_gpu"] = reference_gpu_rate()
     print(json.dumps(line), flush=True)
 
 
@@ -319,6 +340,46 @@ def process_map_leg(args, dev, rank=0, world=1):
                                    "scenarios": [c["scenario"] for c in checks]},
            "clocks": clk.summary(), "error_word": err}
     b.close()
+    return out
+
+
+def ext_leg(args, dev):
+    """Extended physics (phys = 1: Mills k(T), cp(T) with latent heat, the
+    reference's StepTileTask extended branch) on the 8192^2 field: the
+    bench's raster at dt = 0.1 dx^2/alpha (half the baseline step: the
+    conductivity reaches 1.5x the baseline's), one step per launch,
+    per-step Partials, fields resident in HBM."""
+    import torch
+    from hedgehog_lpbf_b200 import params as P
+    from hedgehog_lpbf_b200 import plan as PL
+    from hedgehog_lpbf_b200.solver import Solver
+    torch.cuda.empty_cache()
+    mat, pr = P.benchmark_material_process()
+    dom = P.square_domain(N_SIDE)
+    k = P.make_const(mat, pr, dom, P.dt_fraction(mat, dom, 0.1))
+    n = args.ext_steps
+    plan = PL.raster_for_steps(dom, k.dt, 2 * N_STEPS_TOTAL, V=1.0, hatch=100e-6, n_tracks=10)
+    s = Solver(k, phys=1, device=dev, Tm=mat.Tm)
+    ring = s.new_ring(n)
+    s.advance(plan[:n], ring)                       # warm-up: the laser's first n steps
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        e0.record()
+        s.advance(plan[n:2 * n], ring)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    peak, _ = measured_peaks()
+    cells = dom.nx * dom.ny
+    out = {"value": cells * n / (ms * 1e-3) / 1e9, "unit": "GCell-updates/s",
+           "time_steps": n, "launches": s.launches(n), "ms": ms, "kmult": k.kmult,
+           "dt_s": k.dt, "kernel": "ext_step_kernel (one step per launch, fused reduction)",
+           "roofline": {"bound": "hbm", "achieved": BYTES_PER_UPDATE * cells * n / (ms * 1e-3) / 1e9,
+                        "peak": peak, "unit": "GB/s"},
+           "clocks": clk.summary(), "error_word": s.read_error()}
+    out["roofline"]["frac"] = out["roofline"]["achieved"] / peak
+    del s, ring
     return out
 
 
@@ -567,6 +628,7 @@ def run_b200_arm(args, rank, world, local_rank):
     # exercised by the tests with gloo ranks on CPU, not on several GPUs
     run_sh = args.sharded and (world == 1 or args.shard_ranks)
     sh = sharded_leg(args, dev, rank, world, value / world) if run_sh else None
+    ext = ext_leg(args, dev) if args.ext else None
     pm = None
     if args.process_map:
         pm = process_map_leg(args, dev, rank, world)
@@ -615,6 +677,7 @@ def run_b200_arm(args, rank, world, local_rank):
                         "the neighbouring runs' compute"},
         "gpu_launches": launches * args.steps,
         "f32k": f32k,
+        "ext_physics": ext,
         "process_map": pm,
         "sharded": sh,
         "superstep": ss,
@@ -632,9 +695,9 @@ def run_b200_arm(args, rank, world, local_rank):
         line["cpu_baseline"] = cb
         if N_SIDE == 8192 and not args.no_ref_gpu:
             torch.cuda.empty_cache()
-            rg = reference_gpu_rate(mat, pr, dom, k, plan)
-            if rg:
-                line["ref_gpu"] = rg
+            rg = reference_gpu_rate()
+            line["ref_gpu"] = rg
+            if rg.get("value"):
                 line["speedup_vs_ref_gpu"] = value / rg["value"]
                 line["e2e_speedup_vs_ref_gpu"] = e2e_value / rg["value"]
     print(json.dumps(line), flush=True)
@@ -656,6 +719,9 @@ def main():
                     help="skip the reference GPU task graph baseline")
     ap.add_argument("--no-f32k", dest="f32k", action="store_false",
                     help="skip the FP32 compensated leg")
+    ap.add_argument("--no-ext", dest="ext", action="store_false",
+                    help="skip the extended-physics leg")
+    ap.add_argument("--ext-steps", type=int, default=300)
     ap.add_argument("--no-process-map", dest="process_map", action="store_false",
                     help="skip the batched process-map leg")
     ap.add_argument("--no-sharded", dest="sharded", action="store_false",
@@ -675,9 +741,13 @@ def main():
                     help="grid side (smaller sides are for profiling only)")
     ap.add_argument("--iter-steps", type=int, default=STEPS_PER_ITER,
                     help="time steps per bench step")
+    ap.add_argument("--ref-gpu-child", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
     globals()["N_SIDE"] = args.side
     globals()["STEPS_PER_ITER"] = args.iter_steps
+    if args.ref_gpu_child:
+        print(json.dumps(reference_gpu_child()), flush=True)
+        return
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

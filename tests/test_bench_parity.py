@@ -143,7 +143,7 @@ def test_raster_over_mirror_edges_vs_oracle(gpu, where):
 
 
 def test_process_map_scenarios_full_run_vs_oracle(gpu):
-    """Process-map scenarios 0-3 (2048^2, 1024^2, 256^2 and 512^2 fields with
+    """Process-map scenarios 0-3 (256^2, 256^2, 2048^2 and 1024^2 fields with
     their drawn power, speed, spot and raster) in one batch over the full
     5000 steps; each field and ring against the oracle."""
     from hedgehog_lpbf_b200 import process_map as PM
