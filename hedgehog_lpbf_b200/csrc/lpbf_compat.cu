@@ -17,6 +17,7 @@
 //   lpbf_launch_extract_col     -> one thread per row
 // ---------------------------------------------------------------------------
 #include <algorithm>
+#include <cstring>
 #include <cooperative_groups.h>
 
 #include "lpbf_host.hpp"
@@ -28,44 +29,55 @@ namespace lpbf_b200 {
 
 // ---- extended physics (temperature-dependent IN718 properties) ------------
 // Mills tables, include/params.hpp:67-73 (physical data, identical values).
-__constant__ double c_T_PTS[9]  = {298, 473, 673, 873, 1073, 1273, 1473, 1533, 1609};
-__constant__ double c_K_PTS[9]  = {8.9, 12.9, 15.8, 18.7, 21.9, 25.6, 28.6, 29.3, 29.6};
-__constant__ double c_CP_PTS[9] = {435, 479, 515, 558, 580, 628, 670, 685, 720};
+constexpr double EXT_T_PTS[9]  = {298, 473, 673, 873, 1073, 1273, 1473, 1533, 1609};
+constexpr double EXT_K_PTS[9]  = {8.9, 12.9, 15.8, 18.7, 21.9, 25.6, 28.6, 29.3, 29.6};
+constexpr double EXT_CP_PTS[9] = {435, 479, 515, 558, 580, 628, 670, 685, 720};
 constexpr double T_SOL = 1533.0, T_LIQ = 1609.0, LATENT = 210.0e3;
 constexpr double INV_MUSHY = 1.0 / (T_LIQ - T_SOL);
 
-// The tables in shared memory (lanes index them divergently): temperatures,
-// k, cp, and the reciprocal segment widths.
-struct ExtTab { double t[9], k[9], cp[9], inv[8]; };
+// The clamped piecewise-linear tables of params.hpp:75-89 as ten straight
+// lines y = a + b T, one per temperature segment: segment 0 (T <= 298) and 9
+// (T > 1609) hold the clamped end values, segment j the chord between table
+// points j-1 and j.  The reference evaluates the same chord as
+// y[j-1] + (T - t[j-1]) / (t[j] - t[j-1]) (y[j] - y[j-1]); the line form
+// agrees with it to a few ulp of y.  A cell's segment is the number of table
+// temperatures below T, counted on a 32-bit key of T (ext_key): for T >= 0
+// the key is twice the upper word of T's bit pattern plus one when the lower
+// word is non-zero, and every table temperature (an integer of at most 11
+// significant bits) has a zero lower word, so T > t_j exactly when
+// key(T) > key(t_j); a negative T gets key 0, segment 0, like the
+// reference's clamp, and a NaN the top segment.
+struct ExtLines {
+    double ak[10], bk[10], ac[10], bc[10];
+    unsigned int tkey[9];              // keys of the table temperatures
+    unsigned int sol_key, liq_key;     // of T_SOL and T_LIQ
+    unsigned int pad;
+};
 
-// params.hpp:75-89: clamped piecewise-linear lookup.  The segment comes from
-// seven compares instead of a search loop, and the segment width's
-// reciprocal replaces the division (an ulp-level difference).
-__device__ __forceinline__ int ext_seg(const ExtTab& tb, double T) {
-    int i = 1;
-#pragma unroll
-    for (int j = 1; j < 8; ++j) i += (T > tb.t[j]) ? 1 : 0;
-    return i;
+inline unsigned int host_key(double v) {
+    unsigned long long b;
+    std::memcpy(&b, &v, sizeof(b));
+    return (unsigned int)((b >> 32) << 1) | (unsigned int)((b & 0xffffffffull) != 0);
 }
-__device__ __forceinline__ double ext_interp(const ExtTab& tb, const double* ys, double T, int i) {
-    if (T <= tb.t[0]) return ys[0];
-    if (T >= tb.t[8]) return ys[8];
-    const double f = (T - tb.t[i - 1]) * tb.inv[i - 1];
-    return ys[i - 1] + f * (ys[i] - ys[i - 1]);
-}
-// k_of(T) * k_enh(T, kmult)  (params.hpp:91-105)
-__device__ __forceinline__ double ext_k(const ExtTab& tb, double T, double kmult, double* k_plain) {
-    const double k = ext_interp(tb, tb.k, T, ext_seg(tb, T));
-    if (k_plain) *k_plain = k;
-    if (kmult <= 1.0) return k;
-    const double s = (T <= T_SOL) ? 0.0 : (T >= T_LIQ) ? 1.0 : (T - T_SOL) * INV_MUSHY;
-    return k * (1.0 + (kmult - 1.0) * s);
-}
-// cp_of(T) plus the latent heat spread over the mushy range (params.hpp:106-110)
-__device__ __forceinline__ double ext_cp(const ExtTab& tb, double T) {
-    double c = ext_interp(tb, tb.cp, T, ext_seg(tb, T));
-    if (T >= T_SOL && T <= T_LIQ) c += LATENT * INV_MUSHY;
-    return c;
+
+ExtLines make_ext_lines() {
+    ExtLines L;
+    L.ak[0] = EXT_K_PTS[0];  L.bk[0] = 0.0;
+    L.ac[0] = EXT_CP_PTS[0]; L.bc[0] = 0.0;
+    for (int j = 1; j < 9; ++j) {
+        const double w = EXT_T_PTS[j] - EXT_T_PTS[j - 1];
+        L.bk[j] = (EXT_K_PTS[j] - EXT_K_PTS[j - 1]) / w;
+        L.ak[j] = EXT_K_PTS[j - 1] - L.bk[j] * EXT_T_PTS[j - 1];
+        L.bc[j] = (EXT_CP_PTS[j] - EXT_CP_PTS[j - 1]) / w;
+        L.ac[j] = EXT_CP_PTS[j - 1] - L.bc[j] * EXT_T_PTS[j - 1];
+    }
+    L.ak[9] = EXT_K_PTS[8];  L.bk[9] = 0.0;
+    L.ac[9] = EXT_CP_PTS[8]; L.bc[9] = 0.0;
+    for (int j = 0; j < 9; ++j) L.tkey[j] = host_key(EXT_T_PTS[j]);
+    L.sol_key = host_key(T_SOL);
+    L.liq_key = host_key(T_LIQ);
+    L.pad = 0;
+    return L;
 }
 
 __global__ void reduce_rows_kernel(const double* __restrict__ T, int nx, int ny, double Tm,
@@ -93,8 +105,20 @@ inline cudaError_t launch_finalize(const Partial* parts, int nblocks, int nx, in
     return cudaLaunchKernelEx(&cfg, finalize_cluster_kernel, parts, nblocks, nx, ny, out);
 }
 
+constexpr int EXT_WARPS = 8;       // warps per CTA
+constexpr int EXT_OWN = 30;        // columns a warp owns (lanes 1..30; lanes 0 and 31 halo)
+constexpr int EXT_H = 64;          // rows per task
+constexpr int EXT_PF = 4;          // rows loaded ahead of the one being updated
+
 struct ExtParams {
     StepConst k;
+    ExtLines L;
+    double hx, hy;                 // inv_dx2 / 2, inv_dy2 / 2 (face averages folded in)
+    double r_dsub, Ta4, esig;      // 1/dSub, Tamb^4, eps sigma (0 without radiation)
+    double dt_rho;                 // dt / rho
+    double r2_cut;                 // beyond this r^2 the source is below 2^-80 of its peak
+    int band_lo, band_hi, bandx_lo, bandx_hi;   // cells the source can reach
+    int nstrips, ntasks;
     int bc;
     double T_edge, Tm;
     Partial* ring;
@@ -104,146 +128,211 @@ struct ExtParams {
     long long ref_nparts;
 };
 
-// Blocks of 16 x 16 threads over tiles of 16 x EXT_ROWS cells (each thread
-// owns EXT_ROWS / 16 cells of one column).  The block stages the tile's T
-// plus a one-cell ring (edge neighbours mirrored: the ghost is the centre)
-// and the conductivities k_eff(T) of all of them in shared memory, so each
-// cell's k_eff is evaluated once and read by its four neighbours.  The cell
-// arithmetic follows include/step_task.hpp:144-184, with the divisions by
-// dSub and by rho cp_eff(T) done as multiplications by correctly rounded
-// reciprocals (ulp-level differences).  For the reference's fused-reduce
-// layout (one Partial per 16 x 16 block) a tile writes its result into its
-// first 16 x 16 entry and the neutral element into the others.
-constexpr int EXT_ROWS = 64;
-constexpr int EXT_RPT = EXT_ROWS / 16;          // cells per thread
+// 1/d for the positive, normal d = cp_eff(T) (435..3200): the hardware's
+// approximate FP64 reciprocal refined by two Newton-Raphson steps,
+// r <- r + r (1 - d r), each of which squares the relative error.
+__device__ __forceinline__ double rcp_newton(double d) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+    double e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-d, r, 1.0);
+    return fma(r, e, r);
+}
 
-template <bool REDUCE>
-__global__ void __launch_bounds__(256)
+// The laser's heat input q_in at cell (x, y) (kernels.cu:141 order), zero
+// where r^2 >= r2_cut (below 2^-80 of the peak).  Out of line: the exp code
+// exists once in the binary and holds no registers in the row loop.
+static __device__ __noinline__ double ext_source(int x, int y, const StepConst& k,
+                                                 double r2_cut) {
+    const double xd = __dsub_rn(__dmul_rn((double)x, k.dx), k.x_l);
+    const double yd = __dsub_rn(__dmul_rn((double)y, k.dy), k.y_l);
+    const double r2 = __dadd_rn(__dmul_rn(xd, xd), __dmul_rn(yd, yd));
+    if (r2 >= r2_cut) return 0.0;
+    return k.q_scale * k.peak_S * exp(__dmul_rn(-2.0 * r2, k.inv_r0_sq));
+}
+
+// The ordering key of T (see ExtLines).
+__device__ __forceinline__ unsigned int ext_key(double T) {
+    const unsigned int hi = (unsigned int)__double2hiint(T);
+    const unsigned int lo = (unsigned int)__double2loint(T);
+    const unsigned int k = (hi << 1) | (lo != 0u ? 1u : 0u);
+    return (int)hi < 0 ? 0u : k;
+}
+
+// Segment of a key in the tables; the table keys are read from the kernel's
+// parameter space (the same for every lane).
+__device__ __forceinline__ int ext_seg(unsigned int key, const ExtLines& Lp) {
+    int s = 0;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s += (key > Lp.tkey[j]) ? 1 : 0;
+    return s;
+}
+
+// k_eff(T) = k_of(T) k_enh(T, kmult) (params.hpp:91-105); kp = k_of(T).
+// L: the line tables in shared memory (indexed per lane); Lp: the same
+// in the parameter space (uniform reads).
+template <bool KM>
+__device__ __forceinline__ double ext_keff(double T, unsigned int key, int s, const ExtLines& L,
+                                           const ExtLines& Lp, double kmult, double& kp) {
+    kp = fma(L.bk[s], T, L.ak[s]);
+    if constexpr (!KM) {
+        return kp;
+    } else {
+        const double f = (key <= Lp.sol_key) ? 0.0
+                       : (key >= Lp.liq_key) ? 1.0 : (T - T_SOL) * INV_MUSHY;
+        return kp * fma(kmult - 1.0, f, 1.0);
+    }
+}
+
+// One warp advances one (strip, chunk) task: 30 owned columns (lane l holds
+// column x0 - 1 + l, lanes 0 and 31 the neighbours either side) down H
+// rows.  Each cell's T and k_eff are loaded and evaluated once, when its row
+// enters; a face's flux (k_a + k_b)(T_b - T_a) is computed once, by the
+// cell left of it (x faces, passed to the right neighbour by a shuffle) or
+// above it (y faces, carried to the next row in a register).  Loads of the
+// cells just outside the field are clamped to the edge cell, which makes the
+// edge faces' flux exactly zero: the reference's mirror ghost (ghost =
+// centre).  The cell arithmetic follows include/step_task.hpp:144-184 and
+// src/gpu/kernels.cu:125-147: div(k grad T) on arithmetic-mean faces, the
+// source, convection, radiation and substrate losses, and the update
+// T + dt rhs / (rho cp_eff(T)) with 1/cp_eff by rcp_newton.  Partials as in
+// the baseline kernel: per lane over its column's owned cells, then warps,
+// CTAs and the last CTA.
+template <bool REDUCE, bool KM>
+__global__ void __launch_bounds__(EXT_WARPS * 32, 3)
 ext_step_kernel(const double* __restrict__ Tin, double* __restrict__ Tout,
                 const __grid_constant__ ExtParams p) {
     const StepConst& k = p.k;
-    __shared__ double sT[EXT_ROWS + 2][18], sK[EXT_ROWS + 2][18];
-    __shared__ ExtTab tb;
-    const int tid = threadIdx.y * 16 + threadIdx.x;
+    __shared__ ExtLines L;
+    __shared__ Partial red[EXT_WARPS];
+    __shared__ unsigned int s_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x < (int)(sizeof(ExtLines) / sizeof(double)))
+        reinterpret_cast<double*>(&L)[threadIdx.x] =
+            reinterpret_cast<const double*>(&p.L)[threadIdx.x];
+    __syncthreads();
     const int nx = k.nx, ny = k.ny;
     const long long N = (long long)nx * ny;
-    if (tid < 9) {
-        tb.t[tid] = c_T_PTS[tid];
-        tb.k[tid] = c_K_PTS[tid];
-        tb.cp[tid] = c_CP_PTS[tid];
-        if (tid < 8) tb.inv[tid] = 1.0 / (c_T_PTS[tid + 1] - c_T_PTS[tid]);
-    }
-    __syncthreads();
-    const int bx = blockIdx.x * 16, by = blockIdx.y * EXT_ROWS;
-    for (int e = tid; e < (EXT_ROWS + 2) * 18; e += 256) {
-        const int i = e % 18, j = e / 18;
-        const int gx = min(max(bx + i - 1, 0), nx - 1);
-        const int gy = min(max(by + j - 1, 0), ny - 1);
-        const double T = __ldg(Tin + (size_t)gy * nx + gx);
-        sT[j][i] = T;
-        sK[j][i] = ext_k(tb, T, k.kmult, nullptr);
-    }
-    __syncthreads();
-    const double r_dsub = __drcp_rn(k.dSub);
-    const double Ta4 = k.Tamb * k.Tamb * k.Tamb * k.Tamb;
-    const int tx = threadIdx.x;
-    const int x = bx + tx;
+    const double kmult = k.kmult;
+
     double tm = -1.0;
     long long ag = N;
     int mn = ny, mx = -1;
-#pragma unroll 1
-    for (int q = 0; q < EXT_RPT; ++q) {
-        const int ty = threadIdx.y + 16 * q;            // rows of a thread step by 16
-        const int y = by + ty;
-        if (!(x < nx && y < ny)) continue;
-        const long long c = (long long)y * nx + x;
-        double v;
-        if (p.bc == 1 && (x == 0 || y == 0 || x == nx - 1 || y == ny - 1)) {
-            v = p.T_edge;
-        } else {
-            const double T = sT[ty + 1][tx + 1];
-            const double Txm = sT[ty + 1][tx], Txp = sT[ty + 1][tx + 2];
-            const double Tym = sT[ty][tx + 1], Typ = sT[ty + 2][tx + 1];
-            const double kC = sK[ty + 1][tx + 1];
-            const double kxm = 0.5 * (kC + sK[ty + 1][tx]);
-            const double kxp = 0.5 * (kC + sK[ty + 1][tx + 2]);
-            const double kym = 0.5 * (kC + sK[ty][tx + 1]);
-            const double kyp = 0.5 * (kC + sK[ty + 2][tx + 1]);
-            const double div = (kxp * (Txp - T) - kxm * (T - Txm)) * k.inv_dx2
-                             + (kyp * (Typ - T) - kym * (T - Tym)) * k.inv_dy2;
-            const double xd = __dsub_rn(__dmul_rn((double)x, k.dx), k.x_l);
-            const double yd = __dsub_rn(__dmul_rn((double)y, k.dy), k.y_l);
-            const double r2 = __dadd_rn(__dmul_rn(xd, xd), __dmul_rn(yd, yd));
+    for (int task = blockIdx.x * EXT_WARPS + wid; task < p.ntasks;
+         task += gridDim.x * EXT_WARPS) {
+        const int strip = task % p.nstrips, chunk = task / p.nstrips;
+        const int x = strip * EXT_OWN - 1 + lane;
+        const int xc = min(max(x, 0), nx - 1);
+        const bool owned = lane >= 1 && lane <= EXT_OWN && x < nx;
+        const int y0 = chunk * EXT_H, y1 = min(y0 + EXT_H, ny);
+        const bool src_strip = !(strip * EXT_OWN + EXT_OWN <= p.bandx_lo ||
+                                 strip * EXT_OWN > p.bandx_hi);
+        const double* col = Tin + xc;
+        // rows y0 - 1 (up) and y0 (centre), clamped at the field's edges
+        double Tu = __ldg(col + (size_t)max(y0 - 1, 0) * nx);
+        double Tc = __ldg(col + (size_t)y0 * nx);
+        double kpu;
+        const unsigned int kyu = ext_key(Tu);
+        const double ku = ext_keff<KM>(Tu, kyu, ext_seg(kyu, p.L), L, p.L, kmult, kpu);
+        unsigned int kyc = ext_key(Tc);
+        int sc = ext_seg(kyc, p.L);
+        double kpc;
+        double kc = ext_keff<KM>(Tc, kyc, sc, L, p.L, kmult, kpc);
+        double Fu = __dmul_rn(__dadd_rn(ku, kc), __dsub_rn(Tc, Tu));
+        // the next EXT_PF rows in flight (a global load's latency spans
+        // several rows' arithmetic)
+        double Tq[EXT_PF];
+#pragma unroll
+        for (int i = 0; i < EXT_PF; ++i)
+            Tq[i] = __ldg(col + (size_t)min(y0 + 1 + i, ny - 1) * nx);
+#pragma unroll EXT_PF
+        for (int y = y0; y < y1; ++y) {
+            const double Td = Tq[0];
+#pragma unroll
+            for (int i = 0; i < EXT_PF - 1; ++i) Tq[i] = Tq[i + 1];
+            // row y + EXT_PF + 1 is the lower neighbour of the task's row
+            // y + EXT_PF: needed while that row is < y1
+            Tq[EXT_PF - 1] = (y + EXT_PF < y1)
+                ? __ldg(col + (size_t)min(y + EXT_PF + 1, ny - 1) * nx) : 0.0;
+            const unsigned int kyd = ext_key(Td);
+            const int sd = ext_seg(kyd, p.L);
+            double kpd;
+            const double kd = ext_keff<KM>(Td, kyd, sd, L, p.L, kmult, kpd);
+            // faces: right (this lane) and left (the lane to the left), down
+            const double TR = __shfl_down_sync(0xffffffffu, Tc, 1);
+            const double kR = __shfl_down_sync(0xffffffffu, kc, 1);
+            const double Fr = __dmul_rn(__dadd_rn(kc, kR), __dsub_rn(TR, Tc));
+            const double Fl = __shfl_up_sync(0xffffffffu, Fr, 1);
+            const double Fd = __dmul_rn(__dadd_rn(kc, kd), __dsub_rn(Td, Tc));
+            const double div = fma(__dsub_rn(Fd, Fu), p.hy, __dmul_rn(__dsub_rn(Fr, Fl), p.hx));
             double q_in = 0.0;
-            if (k.q_scale != 0.0 && r2 * k.inv_r0_sq < 0.5 * EXP_CUT)
-                q_in = k.q_scale * k.peak_S * exp(__dmul_rn(-2.0 * r2, k.inv_r0_sq));
-            double q_top = k.hConv * (T - k.Tamb);
-            if (k.radiation) {
-                const double T4 = T * T * T * T;
-                q_top += k.eps * SIGMA_SB * (T4 - Ta4);
+            if (src_strip && y >= p.band_lo && y <= p.band_hi && k.q_scale != 0.0)
+                q_in = ext_source(x, y, k, p.r2_cut);
+            const double T2 = __dmul_rn(Tc, Tc);
+            const double q_top = fma(p.esig, fma(T2, T2, -p.Ta4), k.hConv * (Tc - k.Tamb));
+            const double q_bot = __dmul_rn(kpc * p.r_dsub, Tc - k.Tsub);
+            const double rhs = fma(q_in - (q_top + q_bot), k.inv_h, div);
+            double cp = fma(L.bc[sc], Tc, L.ac[sc]);
+            if (kyc >= p.L.sol_key && kyc <= p.L.liq_key) cp += LATENT * INV_MUSHY;
+            double v = fma(__dmul_rn(rhs, p.dt_rho), rcp_newton(cp), Tc);
+            if (p.bc == 1 && (x == 0 || y == 0 || x == nx - 1 || y == ny - 1)) v = p.T_edge;
+            if (owned) Tout[(size_t)y * nx + x] = v;
+            if constexpr (REDUCE) {
+                // a lane meets its column's cells in increasing index order:
+                // strict '>' keeps the first maximum; NaN never wins
+                if (owned && v > tm) { tm = v; ag = (long long)y * nx + x; }
+                if (__any_sync(0xffffffffu, owned && v > p.Tm) && lane == 0) {
+                    mn = min(mn, y);
+                    mx = max(mx, y);
+                }
             }
-            // one table segment for the substrate conductivity (no kmult) and cp
-            const int sg = ext_seg(tb, T);
-            const double k_plain = k.kmult <= 1.0 ? kC : ext_interp(tb, tb.k, T, sg);
-            double cp = ext_interp(tb, tb.cp, T, sg);
-            if (T >= T_SOL && T <= T_LIQ) cp += LATENT * INV_MUSHY;
-            const double q_bot = (k_plain * r_dsub) * (T - k.Tsub);
-            const double rhs = div + (q_in - q_top - q_bot) * k.inv_h;
-            v = T + (k.dt * rhs) * __drcp_rn(k.rho * cp);
-        }
-        Tout[c] = v;
-        if constexpr (REDUCE) {
-            // rows of this thread come in increasing order: strict '>' keeps
-            // the first (smallest-index) maximum; NaN never wins
-            if (v > tm) { tm = v; ag = c; }
-            if (v > p.Tm) { mn = min(mn, y); mx = max(mx, y); }
+            // shift the rows
+            Fu = Fd;
+            Tc = Td; kc = kd; kpc = kpd; sc = sd; kyc = kyd;
         }
     }
     if constexpr (REDUCE) {
+        mn = __shfl_sync(0xffffffffu, mn, 0);
+        mx = __shfl_sync(0xffffffffu, mx, 0);
         partial_warp_reduce(tm, ag, mn, mx);
-        __shared__ Partial red[8];
-        __shared__ unsigned int s_last;
-        if ((tid & 31) == 0) red[tid >> 5] = Partial{tm, ag, mn, mx};
+        if (lane == 0) red[wid] = Partial{tm, ag, mn, mx};
         __syncthreads();
-        const int nblk = gridDim.x * gridDim.y;
-        if (tid == 0) {
+        if (threadIdx.x == 0) {
             double a = -1.0; long long b = N; int c1 = ny, d1 = -1;
-            for (int w = 0; w < 8; ++w)
+            for (int w = 0; w < EXT_WARPS; ++w)
                 partial_take(a, b, c1, d1, red[w].tmax, red[w].arg, red[w].ymin, red[w].ymax);
-            if (p.ref_out) {
-                // reference layout: 16 x 16 blocks, row-major over the grid
-                const int gx16 = (nx + 15) / 16, gy16 = (ny + 15) / 16;
-                const Partial neutral{-1.0, N, ny, -1};
-                for (int q = 0; q < EXT_RPT; ++q) {
-                    const int yb = blockIdx.y * EXT_RPT + q;
-                    if (yb >= gy16) break;
-                    const long long idx = (long long)yb * gx16 + blockIdx.x;
-                    if (idx < p.ref_nparts) p.ref_out[idx] = q == 0 ? Partial{a, b, c1, d1} : neutral;
-                }
-            } else {
-                p.scratch[blockIdx.y * gridDim.x + blockIdx.x] = Partial{a, b, c1, d1};
-            }
+            if (p.ref_out) p.ref_out[blockIdx.x] = Partial{a, b, c1, d1};
+            else p.scratch[blockIdx.x] = Partial{a, b, c1, d1};
         }
-        if (p.ref_out) return;
+        if (p.ref_out) {
+            // the rest of the caller's entries: the neutral element
+            const Partial neutral{-1.0, N, ny, -1};
+            for (long long i = gridDim.x + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+                 i < p.ref_nparts; i += (long long)gridDim.x * blockDim.x)
+                p.ref_out[i] = neutral;
+            return;
+        }
         __threadfence();
         __syncthreads();
-        if (tid == 0) s_last = (atomicAdd(p.counter, 1u) == (unsigned)nblk - 1) ? 1u : 0u;
+        if (threadIdx.x == 0)
+            s_last = (atomicAdd(p.counter, 1u) == gridDim.x - 1) ? 1u : 0u;
         __syncthreads();
         if (!s_last) return;
         __threadfence();
         double a = -1.0; long long b = N; int c1 = ny, d1 = -1;
-        for (int i = tid; i < nblk; i += 256) {
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
             const Partial* qq = &p.scratch[i];
             partial_take(a, b, c1, d1, __ldcg(&qq->tmax), __ldcg(&qq->arg), __ldcg(&qq->ymin),
                          __ldcg(&qq->ymax));
         }
         partial_warp_reduce(a, b, c1, d1);
         __syncthreads();
-        if ((tid & 31) == 0) red[tid >> 5] = Partial{a, b, c1, d1};
+        if (lane == 0) red[wid] = Partial{a, b, c1, d1};
         __syncthreads();
-        if (tid == 0) {
+        if (threadIdx.x == 0) {
             double a2 = -1.0; long long b2 = N; int c2 = ny, d2 = -1;
-            for (int w = 0; w < 8; ++w)
+            for (int w = 0; w < EXT_WARPS; ++w)
                 partial_take(a2, b2, c2, d2, red[w].tmax, red[w].arg, red[w].ymin, red[w].ymax);
             p.ring[0] = Partial{a2, b2, c2, d2};
             *p.counter = 0u;
@@ -251,30 +340,51 @@ ext_step_kernel(const double* __restrict__ Tin, double* __restrict__ Tout,
     }
 }
 
+template <bool REDUCE>
+cudaError_t launch_ext_t(bool km, int grid, const double* Tin, double* Tout, const ExtParams& p,
+                         cudaStream_t stream) {
+    if (km) ext_step_kernel<REDUCE, true><<<grid, EXT_WARPS * 32, 0, stream>>>(Tin, Tout, p);
+    else ext_step_kernel<REDUCE, false><<<grid, EXT_WARPS * 32, 0, stream>>>(Tin, Tout, p);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_ext_step(const double* Tin, double* Tout, const StepConst& k, int bc,
                             double T_edge, double Tm, Partial* ring, Workspace* ws,
                             Partial* ref_out, long long ref_nparts, cudaStream_t stream) {
-    ExtParams p{};
-    p.k = k; p.bc = bc; p.T_edge = T_edge; p.Tm = Tm;
+    static const ExtLines lines = make_ext_lines();
+    ExtParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.k = k; p.L = lines;
+    p.hx = 0.5 * k.inv_dx2;
+    p.hy = 0.5 * k.inv_dy2;
+    p.r_dsub = 1.0 / k.dSub;
+    p.Ta4 = k.Tamb * k.Tamb * k.Tamb * k.Tamb;
+    p.esig = k.radiation ? k.eps * SIGMA_SB : 0.0;
+    p.dt_rho = k.dt / k.rho;
+    p.bc = bc; p.T_edge = T_edge; p.Tm = Tm;
     p.ring = ring; p.ref_out = ref_out; p.ref_nparts = ref_nparts;
-    const dim3 blk(16, 16);
-    const dim3 grd((k.nx + 15) / 16, (k.ny + EXT_ROWS - 1) / EXT_ROWS);
+    // the source's reach: rows and columns where r^2 < r2_cut (a superset)
+    const Coef c = make_coef(k, bc, T_edge, Tm);
+    const LaserSub las = make_laser(k, k.x_l, k.y_l, k.q_scale);
+    p.r2_cut = c.r2_cut;
+    laser_band(c, &las, 1, &p.band_lo, &p.band_hi, &p.bandx_lo, &p.bandx_hi);
+    p.nstrips = (k.nx + EXT_OWN - 1) / EXT_OWN;
+    p.ntasks = p.nstrips * ((k.ny + EXT_H - 1) / EXT_H);
+    int grid = (p.ntasks + EXT_WARPS - 1) / EXT_WARPS;
+    const bool km = k.kmult > 1.0;
     const bool reduce = ring || ref_out;
-    if (reduce && !ref_out) {
+    if (ref_out) {
+        grid = (int)std::max<long long>(1, std::min<long long>(grid, ref_nparts));
+        return launch_ext_t<true>(km, grid, Tin, Tout, p, stream);
+    }
+    if (reduce) {
         if (!ws) return cudaErrorInvalidValue;
-        if ((long long)grd.x * grd.y > (long long)MAX_CTAS * KMAX) {
-            // more blocks than partial slots: step, then reduce rows separately
-            ext_step_kernel<false><<<grd, blk, 0, stream>>>(Tin, Tout, p);
-            const int nb = std::min(MAX_CTAS * KMAX, k.ny);
-            reduce_rows_kernel<<<nb, 256, 0, stream>>>(Tout, k.nx, k.ny, Tm, ws->parts);
-            return launch_finalize(ws->parts, nb, k.nx, k.ny, ring, stream);
-        }
+        grid = std::min(grid, MAX_CTAS * KMAX);
         p.scratch = ws->parts;
         p.counter = &ws->counter;
+        return launch_ext_t<true>(km, grid, Tin, Tout, p, stream);
     }
-    if (reduce) ext_step_kernel<true><<<grd, blk, 0, stream>>>(Tin, Tout, p);
-    else        ext_step_kernel<false><<<grd, blk, 0, stream>>>(Tin, Tout, p);
-    return cudaGetLastError();
+    return launch_ext_t<false>(km, grid, Tin, Tout, p, stream);
 }
 
 // ---- standalone reduce --------------------------------------------------------

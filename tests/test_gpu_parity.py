@@ -153,6 +153,34 @@ def test_extended_physics_vs_oracle(gpu):
         check_partials(ring_to_numpy(ring), ring_ref, T_ref, 96)
 
 
+@pytest.mark.parametrize("kmult", [1.0, 2.5])
+@pytest.mark.parametrize("bc", [0, 1])
+def test_extended_physics_table_segments_vs_oracle(gpu, kmult, bc):
+    """Extended physics on a field whose cells sit in every segment of the
+    Mills tables, on the table temperatures themselves and on both ends of
+    the mushy range (where k_enh and the latent heat switch), with the laser
+    crossing strip and row-chunk boundaries: every step against the oracle."""
+    from hedgehog_lpbf_b200.solver import ring_to_numpy
+    nx, ny = 301, 203
+    mat, pr, dom, k = bench_const(nx, ny)
+    k.kmult = kmult
+    k.dt = 0.25 * k.dt              # stable for k up to 2.5 x 29.6 W/m/K
+    rng = np.random.default_rng(int(kmult * 10) + bc)
+    T0 = rng.uniform(250.0, 2600.0, size=nx * ny)
+    pts = np.array([298, 473, 673, 873, 1073, 1273, 1473, 1533, 1609], dtype=np.float64)
+    idx = rng.choice(nx * ny, size=4 * len(pts), replace=False)
+    T0[idx] = np.concatenate([pts, np.nextafter(pts, 0.0), np.nextafter(pts, 1e9), pts + 0.5])
+    n = 12
+    las = np.stack([np.linspace(0.05, 0.95, n) * dom.Lx, np.linspace(0.3, 0.6, n) * dom.Ly,
+                    (np.arange(n) % 5 != 4).astype(float)], axis=1)
+    T_ref, ring_ref = O.run(T0, k, las, phys=1, bc=bc, T_D=300.0, Tm=mat.Tm)
+    s = solver(k, phys=1, bc=bc, T_edge=300.0, Tm=mat.Tm, T0=T0)
+    ring = s.new_ring(n)
+    T = s.advance(tick_plan(las), ring).cpu().numpy()
+    assert rel_err(T, T_ref) <= RTOL
+    check_partials(ring_to_numpy(ring), ring_ref, T_ref, nx)
+
+
 # ---- the reference's five launch wrappers ---------------------------------
 
 def _stream():
