@@ -77,12 +77,16 @@ def measured_peaks():
     return 6650.0, "fallback (no MEASURED_PEAKS.json: earlier copy-bandwidth measurement on B200)"
 
 
-# ncu counters of one full-size launch of the dominant kernel (8192^2, depth
-# 3, the bench's own command), summarised with the command that produced
-# them in profiles/advance_kernel_8192.md.  Per launch: DRAM bytes read +
-# written, and the FP64 pipe's share of active cycles.
+# ncu counters of the dominant kernel, summarised with the commands that
+# produced them in profiles/advance_kernel_8192.md: DRAM bytes read +
+# written per full-size launch (8192^2, depth 3, two consecutive launches of
+# the bench's own command with --cache-control none, so a launch also pays
+# the write-back of the previous launch's dirty lines: the steady state),
+# and the FP64 pipe's share of active cycles (4096^2 --set full capture of
+# the same kernel).
 ADVANCE_PROFILE = {
-    3: {"dram_bytes": None, "fp64_pipe": None, "launch_us": None,
+    3: {"dram_bytes": 1.13944e9, "dram_read_bytes": 0.60274e9, "dram_write_bytes": 0.53670e9,
+        "fp64_pipe": 0.539, "issue_active": 0.495, "limiter": "fp64_pipe_latency",
         "source": "profiles/advance_kernel_8192.md"},
 }
 
@@ -208,28 +212,31 @@ def reference_gpu_rate(timeout_s: float = 600.0):
     return {"unavailable": f"reference GPU task graph exited {r.returncode}: {tail[0][:200]}"}
 
 
-def reference_gpu_child(n1: int = 192, n2: int = 1216):
+def reference_gpu_child():
     """The reference's own GPU path on this GPU: its GpuStepTask graph
     (include/gpu_step_task.hpp, run as run_one_row does, hh_gpu_main.cpp:171-
     207) with its kernels (src/gpu/kernels.cu built for sm_100a), default
     options (mode 2, batch 64, unfused, pageable staging) and with the fused
     step+reduce kernel, over the bench's raster plan.  Steady-state rate from
-    two run lengths (the task's device set-up cancels in the difference)."""
+    two run lengths (the task's device set-up cancels in the difference);
+    the fused form finalizes 262,144 per-block partials on one thread per
+    step (34 ms), so it is sampled over fewer steps."""
     from oracle import oracle as O
     mat, pr, dom, k, plan = workload(0)
     if not O.have_reference():
         return {"unavailable": "oracle/_ref (the reference built from its sources) is absent"}
     out = {"unit": "GCell-updates/s", "kind": "reference",
            "what": "reference GpuStepTask graph (mode 2, batch 64) with its own kernels "
-                   "(kernels.cu built for sm_100a), wall clock, "
-                   f"({n2} - {n1}) steps of {dom.nx}x{dom.ny} on the bench's raster"}
+                   f"(kernels.cu built for sm_100a), wall clock, {dom.nx}x{dom.ny} on the "
+                   "bench's raster"}
     with ClockSampler(0) as clk:
-        for name, fused in (("unfused", False), ("fused", True)):
+        for name, fused, n1, n2 in (("unfused", False, 192, 1216), ("fused", True, 64, 192)):
             O.ref_gpu_task_run(k, dom, plan[:64], mat.Tm, pr.Tamb, fused=fused)     # warm-up
             t1, _ = O.ref_gpu_task_run(k, dom, plan[:n1], mat.Tm, pr.Tamb, fused=fused)
             t2, pk = O.ref_gpu_task_run(k, dom, plan[:n2], mat.Tm, pr.Tamb, fused=fused)
             out[name] = {"value": dom.nx * dom.ny * (n2 - n1) / ((t2 - t1) * 1e-3) / 1e9,
-                         "ms_per_step": (t2 - t1) / (n2 - n1), "peak_T_K": pk}
+                         "ms_per_step": (t2 - t1) / (n2 - n1), "peak_T_K": pk,
+                         "steps": f"{n2} - {n1}"}
     out["value"] = max(out["unfused"]["value"], out["fused"]["value"])
     out["clocks"] = clk.summary()
     return out
@@ -465,6 +472,10 @@ def superstep_leg(args, dev):
                           "worst_window_K": hyb["worst_K"]},
         "heldout": rec.get("heldout_trained") if rec else None,
     }
+    del s, Tp, Th
+    if args.ss_scenarios > 0:
+        out["hybrid_process_map"] = hybrid_scenarios(net, args.ss_scenarios, args.ss_pm_steps,
+                                                     dev)
     peak = None
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
@@ -475,6 +486,49 @@ def superstep_leg(args, dev):
     else:   # earlier cuBLAS bf16 burst measurement on B200
         out["forward_4096sq"]["frac_of_fallback_bf16_1590"] = out["forward_4096sq"]["tflops"] / 1590.0
     return out
+
+
+def hybrid_scenarios(net, n_scen: int, n_steps: int, dev):
+    """The batched part of the surrogate-in-the-loop workload: n_scen seeded
+    process-map scenarios (grid side 256..2048, power, speed, spot, raster
+    angle and hatch drawn per scenario), each advanced n_steps by super-steps
+    of the network with the FP64 judge every 8 super-steps (one scenario
+    after another), against the same scenarios advanced together by the
+    batched FP64 kernel (one launch sequence): time-to-solution, max |dT|
+    and melt-area error against the FP64 fields."""
+    import torch
+    from hedgehog_lpbf_b200 import process_map as PM
+    from hedgehog_lpbf_b200.batch import Batch, batch_opts
+    from hedgehog_lpbf_b200.superstep import run_hybrid
+    torch.cuda.empty_cache()
+    scs = PM.process_map(n_scen, n_steps)
+    b = Batch(scs, n_steps, opts=batch_opts(depth=2), device=dev, rings=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.run(0, n_steps)
+    e1.record()
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    hyb_ms, worst, area_worst, judged, rolled = 0.0, 0.0, 0.0, 0, 0
+    for i, sc in enumerate(scs):
+        Th, r = run_hybrid(net, sc.k, sc.plan, np.full(sc.k.nx * sc.k.ny, sc.k.Tamb), n_steps,
+                           judge_every=8, tol_K=5.0, area_tol=0.02, Tm=sc.Tm, device=dev)
+        hyb_ms += r["gpu_ms"]
+        judged += r["judged"]
+        rolled += r["rolled_back"]
+        Tp = b.field(i)
+        worst = max(worst, float((Th - Tp).abs().max().item()))
+        mp, mh = int((Tp > sc.Tm).sum().item()), int((Th > sc.Tm).sum().item())
+        area_worst = max(area_worst, abs(mh - mp) / max(mp, 1) if (mp or mh) else 0.0)
+        del Th
+    b.close()
+    return {"scenarios": n_scen, "steps_each": n_steps, "hybrid_ms": hyb_ms,
+            "plain_fp64_batched_ms": plain_ms, "speedup_vs_plain": plain_ms / hyb_ms,
+            "max_abs_err_vs_fp64_K": worst, "worst_melt_area_err": area_worst,
+            "judged": judged, "rolled_back": rolled,
+            "note": "hybrid scenarios run one after another; the FP64 reference is the "
+                    "batched kernel over all scenarios"}
 
 
 def sharded_leg(args, dev, rank=0, world=1, single_value=None):
@@ -733,8 +787,12 @@ def main():
     ap.add_argument("--pm-steps", type=int, default=5000)
     ap.add_argument("--no-superstep", dest="superstep", action="store_false",
                     help="skip the learned super-stepper leg")
-    ap.add_argument("--ss-steps", type=int, default=4096,
+    ap.add_argument("--ss-steps", type=int, default=20480,
                     help="steps of the 4096^2 raster run by the hybrid (multiple of 128)")
+    ap.add_argument("--ss-scenarios", type=int, default=64,
+                    help="process-map scenarios of the batched hybrid part (0 = skip)")
+    ap.add_argument("--ss-pm-steps", type=int, default=1024,
+                    help="steps of each scenario in the batched hybrid part")
     ap.add_argument("--tune-cache", default=None,
                     help="JSON cache of the batch autotuner (default: tune every run)")
     ap.add_argument("--side", type=int, default=N_SIDE,

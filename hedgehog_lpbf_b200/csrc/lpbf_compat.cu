@@ -106,7 +106,8 @@ inline cudaError_t launch_finalize(const Partial* parts, int nblocks, int nx, in
 }
 
 constexpr int EXT_WARPS = 8;       // warps per CTA
-constexpr int EXT_OWN = 30;        // columns a warp owns (lanes 1..30; lanes 0 and 31 halo)
+constexpr int EXT_V = 2;           // columns per lane
+constexpr int EXT_OWN = 32 * EXT_V - 2;   // columns a warp owns (the first and last are halo)
 constexpr int EXT_H = 64;          // rows per task
 constexpr int EXT_PF = 4;          // rows loaded ahead of the one being updated
 
@@ -185,22 +186,60 @@ __device__ __forceinline__ double ext_keff(double T, unsigned int key, int s, co
     }
 }
 
-// One warp advances one (strip, chunk) task: 30 owned columns (lane l holds
-// column x0 - 1 + l, lanes 0 and 31 the neighbours either side) down H
-// rows.  Each cell's T and k_eff are loaded and evaluated once, when its row
-// enters; a face's flux (k_a + k_b)(T_b - T_a) is computed once, by the
-// cell left of it (x faces, passed to the right neighbour by a shuffle) or
-// above it (y faces, carried to the next row in a register).  Loads of the
+// A cell as the row stream carries it: T, k_eff(T), k_of(T) (the substrate
+// loss uses the conductivity without kmult), its ordering key and segment.
+struct ExtCell { double T, k, kp; unsigned int key; int seg; };
+
+template <bool KM>
+__device__ __forceinline__ ExtCell ext_cell(double T, const ExtLines& L, const ExtLines& Lp,
+                                            double kmult) {
+    ExtCell c;
+    c.T = T;
+    c.key = ext_key(T);
+    c.seg = ext_seg(c.key, Lp);
+    c.k = ext_keff<KM>(T, c.key, c.seg, L, Lp, kmult, c.kp);
+    return c;
+}
+
+// Flux through the face between cells a and b, (k_a + k_b)(T_b - T_a) (twice
+// the arithmetic-mean face conductivity times the difference; the 1/2 is in
+// hx, hy).
+__device__ __forceinline__ double ext_flux(const ExtCell& a, const ExtCell& b) {
+    return __dmul_rn(__dadd_rn(a.k, b.k), __dsub_rn(b.T, a.T));
+}
+
+// The new temperature of cell c from div(k grad T) and the source:
+// T + dt (div + (q_in - q_top - q_bot) / h) / (rho cp_eff(T)).
+__device__ __forceinline__ double ext_update(const ExtCell& c, double div, double q_in,
+                                             const StepConst& k, const ExtParams& p,
+                                             const ExtLines& L) {
+    const double T = c.T;
+    const double T2 = __dmul_rn(T, T);
+    const double q_top = fma(p.esig, fma(T2, T2, -p.Ta4), k.hConv * (T - k.Tamb));
+    const double q_bot = __dmul_rn(c.kp * p.r_dsub, T - k.Tsub);
+    const double rhs = fma(q_in - (q_top + q_bot), k.inv_h, div);
+    double cp = fma(L.bc[c.seg], T, L.ac[c.seg]);
+    if (c.key >= p.L.sol_key && c.key <= p.L.liq_key) cp += LATENT * INV_MUSHY;
+    return fma(__dmul_rn(rhs, p.dt_rho), rcp_newton(cp), T);
+}
+
+// One warp advances one (strip, chunk) task: 62 owned columns (lane l holds
+// the two columns xs + 2l and xs + 2l + 1; lane 0's first and lane 31's
+// second are the neighbours either side) down H rows.  Each cell's T and
+// k_eff are loaded and evaluated once, when its row enters; a face's flux
+// (k_a + k_b)(T_b - T_a) is computed once, inside the lane, by the lane to
+// its left (passed on by a shuffle) or by the cell above it (y faces,
+// carried to the next row in registers).  Loads of the
 // cells just outside the field are clamped to the edge cell, which makes the
 // edge faces' flux exactly zero: the reference's mirror ghost (ghost =
 // centre).  The cell arithmetic follows include/step_task.hpp:144-184 and
 // src/gpu/kernels.cu:125-147: div(k grad T) on arithmetic-mean faces, the
 // source, convection, radiation and substrate losses, and the update
 // T + dt rhs / (rho cp_eff(T)) with 1/cp_eff by rcp_newton.  Partials as in
-// the baseline kernel: per lane over its column's owned cells, then warps,
-// CTAs and the last CTA.
+// the baseline kernel: per lane over its owned cells, then warps, CTAs and
+// the last CTA.
 template <bool REDUCE, bool KM>
-__global__ void __launch_bounds__(EXT_WARPS * 32, 3)
+__global__ void __launch_bounds__(EXT_WARPS * 32, 2)
 ext_step_kernel(const double* __restrict__ Tin, double* __restrict__ Tout,
                 const __grid_constant__ ExtParams p) {
     const StepConst& k = p.k;
@@ -222,74 +261,88 @@ ext_step_kernel(const double* __restrict__ Tin, double* __restrict__ Tout,
     for (int task = blockIdx.x * EXT_WARPS + wid; task < p.ntasks;
          task += gridDim.x * EXT_WARPS) {
         const int strip = task % p.nstrips, chunk = task / p.nstrips;
-        const int x = strip * EXT_OWN - 1 + lane;
-        const int xc = min(max(x, 0), nx - 1);
-        const bool owned = lane >= 1 && lane <= EXT_OWN && x < nx;
+        // lane l holds columns xa = xs + 2l and xb = xa + 1; the warp owns
+        // xs + 1 .. xs + EXT_OWN (lane 0's a and lane 31's b are its halo)
+        const int xs = strip * EXT_OWN - 1;
+        const int xa = xs + EXT_V * lane, xb = xa + 1;
+        const int ca = min(max(xa, 0), nx - 1), cb = min(max(xb, 0), nx - 1);
+        const bool own_a = lane >= 1 && xa < nx;
+        const bool own_b = lane <= 30 && xb < nx;
         const int y0 = chunk * EXT_H, y1 = min(y0 + EXT_H, ny);
-        const bool src_strip = !(strip * EXT_OWN + EXT_OWN <= p.bandx_lo ||
-                                 strip * EXT_OWN > p.bandx_hi);
-        const double* col = Tin + xc;
+        const bool src_strip = !(xs + 1 + EXT_OWN <= p.bandx_lo || xs + 1 > p.bandx_hi);
         // rows y0 - 1 (up) and y0 (centre), clamped at the field's edges
-        double Tu = __ldg(col + (size_t)max(y0 - 1, 0) * nx);
-        double Tc = __ldg(col + (size_t)y0 * nx);
-        double kpu;
-        const unsigned int kyu = ext_key(Tu);
-        const double ku = ext_keff<KM>(Tu, kyu, ext_seg(kyu, p.L), L, p.L, kmult, kpu);
-        unsigned int kyc = ext_key(Tc);
-        int sc = ext_seg(kyc, p.L);
-        double kpc;
-        double kc = ext_keff<KM>(Tc, kyc, sc, L, p.L, kmult, kpc);
-        double Fu = __dmul_rn(__dadd_rn(ku, kc), __dsub_rn(Tc, Tu));
+        ExtCell ua, ub, a, b;
+        {
+            const size_t ru = (size_t)max(y0 - 1, 0) * nx, rc = (size_t)y0 * nx;
+            ua = ext_cell<KM>(__ldg(Tin + ru + ca), L, p.L, kmult);
+            ub = ext_cell<KM>(__ldg(Tin + ru + cb), L, p.L, kmult);
+            a = ext_cell<KM>(__ldg(Tin + rc + ca), L, p.L, kmult);
+            b = ext_cell<KM>(__ldg(Tin + rc + cb), L, p.L, kmult);
+        }
+        double Fua = ext_flux(ua, a), Fub = ext_flux(ub, b);
         // the next EXT_PF rows in flight (a global load's latency spans
         // several rows' arithmetic)
-        double Tq[EXT_PF];
+        double Qa[EXT_PF], Qb[EXT_PF];
 #pragma unroll
-        for (int i = 0; i < EXT_PF; ++i)
-            Tq[i] = __ldg(col + (size_t)min(y0 + 1 + i, ny - 1) * nx);
+        for (int i = 0; i < EXT_PF; ++i) {
+            const size_t r = (size_t)min(y0 + 1 + i, ny - 1) * nx;
+            Qa[i] = __ldg(Tin + r + ca);
+            Qb[i] = __ldg(Tin + r + cb);
+        }
 #pragma unroll EXT_PF
         for (int y = y0; y < y1; ++y) {
-            const double Td = Tq[0];
+            const double Tda = Qa[0], Tdb = Qb[0];
 #pragma unroll
-            for (int i = 0; i < EXT_PF - 1; ++i) Tq[i] = Tq[i + 1];
+            for (int i = 0; i < EXT_PF - 1; ++i) { Qa[i] = Qa[i + 1]; Qb[i] = Qb[i + 1]; }
             // row y + EXT_PF + 1 is the lower neighbour of the task's row
             // y + EXT_PF: needed while that row is < y1
-            Tq[EXT_PF - 1] = (y + EXT_PF < y1)
-                ? __ldg(col + (size_t)min(y + EXT_PF + 1, ny - 1) * nx) : 0.0;
-            const unsigned int kyd = ext_key(Td);
-            const int sd = ext_seg(kyd, p.L);
-            double kpd;
-            const double kd = ext_keff<KM>(Td, kyd, sd, L, p.L, kmult, kpd);
-            // faces: right (this lane) and left (the lane to the left), down
-            const double TR = __shfl_down_sync(0xffffffffu, Tc, 1);
-            const double kR = __shfl_down_sync(0xffffffffu, kc, 1);
-            const double Fr = __dmul_rn(__dadd_rn(kc, kR), __dsub_rn(TR, Tc));
-            const double Fl = __shfl_up_sync(0xffffffffu, Fr, 1);
-            const double Fd = __dmul_rn(__dadd_rn(kc, kd), __dsub_rn(Td, Tc));
-            const double div = fma(__dsub_rn(Fd, Fu), p.hy, __dmul_rn(__dsub_rn(Fr, Fl), p.hx));
-            double q_in = 0.0;
-            if (src_strip && y >= p.band_lo && y <= p.band_hi && k.q_scale != 0.0)
-                q_in = ext_source(x, y, k, p.r2_cut);
-            const double T2 = __dmul_rn(Tc, Tc);
-            const double q_top = fma(p.esig, fma(T2, T2, -p.Ta4), k.hConv * (Tc - k.Tamb));
-            const double q_bot = __dmul_rn(kpc * p.r_dsub, Tc - k.Tsub);
-            const double rhs = fma(q_in - (q_top + q_bot), k.inv_h, div);
-            double cp = fma(L.bc[sc], Tc, L.ac[sc]);
-            if (kyc >= p.L.sol_key && kyc <= p.L.liq_key) cp += LATENT * INV_MUSHY;
-            double v = fma(__dmul_rn(rhs, p.dt_rho), rcp_newton(cp), Tc);
-            if (p.bc == 1 && (x == 0 || y == 0 || x == nx - 1 || y == ny - 1)) v = p.T_edge;
-            if (owned) Tout[(size_t)y * nx + x] = v;
+            if (y + EXT_PF < y1) {
+                const size_t r = (size_t)min(y + EXT_PF + 1, ny - 1) * nx;
+                Qa[EXT_PF - 1] = __ldg(Tin + r + ca);
+                Qb[EXT_PF - 1] = __ldg(Tin + r + cb);
+            }
+            const ExtCell da = ext_cell<KM>(Tda, L, p.L, kmult);
+            const ExtCell db = ext_cell<KM>(Tdb, L, p.L, kmult);
+            // x faces: a|b inside the lane, b|next lane's a, and the previous
+            // lane's b|a as this lane's left face; y faces: down, carried up
+            const double Fab = ext_flux(a, b);
+            const double TR = __shfl_down_sync(0xffffffffu, a.T, 1);
+            const double kR = __shfl_down_sync(0xffffffffu, a.k, 1);
+            const double FbR = __dmul_rn(__dadd_rn(b.k, kR), __dsub_rn(TR, b.T));
+            const double FLa = __shfl_up_sync(0xffffffffu, FbR, 1);
+            const double Fda = ext_flux(a, da), Fdb = ext_flux(b, db);
+            const double diva = fma(__dsub_rn(Fda, Fua), p.hy, __dmul_rn(__dsub_rn(Fab, FLa), p.hx));
+            const double divb = fma(__dsub_rn(Fdb, Fub), p.hy, __dmul_rn(__dsub_rn(FbR, Fab), p.hx));
+            double qa = 0.0, qb = 0.0;
+            if (src_strip && y >= p.band_lo && y <= p.band_hi && k.q_scale != 0.0) {
+                qa = ext_source(xa, y, k, p.r2_cut);
+                qb = ext_source(xb, y, k, p.r2_cut);
+            }
+            double va = ext_update(a, diva, qa, k, p, L);
+            double vb = ext_update(b, divb, qb, k, p, L);
+            if (p.bc == 1) {
+                const bool ey = y == 0 || y == ny - 1;
+                if (ey || xa == 0 || xa == nx - 1) va = p.T_edge;
+                if (ey || xb == 0 || xb == nx - 1) vb = p.T_edge;
+            }
+            double* row = Tout + (size_t)y * nx;
+            if (own_a) row[xa] = va;
+            if (own_b) row[xb] = vb;
             if constexpr (REDUCE) {
-                // a lane meets its column's cells in increasing index order:
-                // strict '>' keeps the first maximum; NaN never wins
-                if (owned && v > tm) { tm = v; ag = (long long)y * nx + x; }
-                if (__any_sync(0xffffffffu, owned && v > p.Tm) && lane == 0) {
+                // a lane meets its cells in increasing index order (rows
+                // down, a before b): strict '>' keeps the first maximum; NaN
+                // never wins
+                if (own_a && va > tm) { tm = va; ag = (long long)y * nx + xa; }
+                if (own_b && vb > tm) { tm = vb; ag = (long long)y * nx + xb; }
+                if (__any_sync(0xffffffffu, (own_a && va > p.Tm) || (own_b && vb > p.Tm)) &&
+                    lane == 0) {
                     mn = min(mn, y);
                     mx = max(mx, y);
                 }
             }
             // shift the rows
-            Fu = Fd;
-            Tc = Td; kc = kd; kpc = kpd; sc = sd; kyc = kyd;
+            Fua = Fda; Fub = Fdb;
+            a = da; b = db;
         }
     }
     if constexpr (REDUCE) {

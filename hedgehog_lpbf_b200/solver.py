@@ -68,8 +68,12 @@ class Solver:
         return self.bufs[self.cur]
 
     def set_field(self, T0) -> None:
+        """A scalar, a host array, or a tensor (a device tensor is copied on
+        the device, stream-ordered, with no host synchronization)."""
         if np.isscalar(T0):
             self.bufs[self.cur].fill_(float(T0))
+        elif isinstance(T0, torch.Tensor):
+            self.bufs[self.cur].copy_(T0.reshape(self.ny, self.nx))
         else:
             src = torch.as_tensor(np.asarray(T0, dtype=np.float64).reshape(self.ny, self.nx))
             self.bufs[self.cur].copy_(src)

@@ -163,65 +163,100 @@ def judge(got: torch.Tensor, ref: torch.Tensor, tol_K: float, area_tol: float, T
     """The FP64 judge's verdict on one window: (max |got - ref| in K, melt-pool
     area error, roll back?).  Roll back where the field misses by more than
     tol_K or the area of T > Tm differs by more than area_tol (relative)."""
-    diff = float((got - ref).abs().max().item())
-    a_ref = int((ref > Tm).sum().item())
-    a_got = int((got > Tm).sum().item())
-    area = abs(a_got - a_ref) / max(a_ref, 1) if (a_ref or a_got) else 0.0
-    return diff, area, (diff > tol_K or area > area_tol or not math.isfinite(diff))
+    diff, area, back = judge_device(got, ref, tol_K, area_tol, Tm)
+    return float(diff.item()), float(area.item()), bool(back.item())
+
+
+def judge_device(got: torch.Tensor, ref: torch.Tensor, tol_K: float, area_tol: float,
+                 Tm: float):
+    """``judge`` as 0-d device tensors, with no host synchronization: the
+    loop below acts on the verdict on the device (torch.where) and reads the
+    records once at the end."""
+    diff = (got - ref).abs().max()
+    a_ref = (ref > Tm).sum()
+    a_got = (got > Tm).sum()
+    area = (a_got - a_ref).abs().double() / a_ref.clamp(min=1).double()
+    back = (diff > tol_K) | (area > area_tol) | ~torch.isfinite(diff)
+    return diff, area, back
+
+
+def _windows(plan, blocks: int, per_block: int, k, margin: int, halo: int):
+    """Per judged block: the laser window (rows y0:y1, columns x0:x1, the
+    cells the judge compares) and the origin of a fixed-size FP64 solve box
+    that holds it with `halo` cells of surroundings (fewer at the field's
+    edges, which are the field's own boundary).  Returns (windows, box
+    height, box width)."""
+    win = [_window(plan, b * per_block, (b + 1) * per_block, k, margin, k.nx, k.ny)
+           for b in range(blocks)]
+    bh = min(k.ny, max(w[1] - w[0] for w in win) + 2 * halo)
+    bw = min(k.nx, max(w[3] - w[2] for w in win) + 2 * halo)
+    out = []
+    for wy0, wy1, wx0, wx1 in win:
+        oy = min(max(wy0 - halo, 0), k.ny - bh)
+        ox = min(max(wx0 - halo, 0), k.nx - bw)
+        out.append((wy0, wy1, wx0, wx1, oy, ox))
+    return out, bh, bw
 
 
 def run_hybrid(net: Net, k, plan, T0, n_steps: int, judge_every: int = 8, tol_K: float = 5.0,
                area_tol: float = 0.02, Tm: float = 1700.0, margin: int | None = None,
                halo: int = 32, device="cuda:0"):
     """Super-steps of the network with the FP64 judge and rollback.  Returns
-    (field, record)."""
+    (field, record).
+
+    Every ``judge_every`` super-steps the FP64 solver re-advances, from the
+    block's start, a fixed-size box around the block's laser window (one
+    solver for the whole run, so no buffers, workspace or tensor map are
+    made per window); the verdict and the rollback (torch.where over the
+    window) stay on the device, and the per-window records are read once at
+    the end."""
     dev = torch.device(device)
-    T = torch.as_tensor(np.asarray(T0, dtype=np.float64)).to(dev).reshape(k.ny, k.nx).clone()
+    if isinstance(T0, torch.Tensor):
+        T = T0.to(dev, torch.float64).reshape(k.ny, k.nx).clone()
+    else:
+        T = torch.as_tensor(np.asarray(T0, dtype=np.float64)).to(dev).reshape(k.ny, k.nx).clone()
     if margin is None:
         margin = int(math.ceil(6.0 / math.sqrt(k.inv_r0_sq) / k.dx)) + 8
-    blocks = n_steps // (STEPS * judge_every)
-    rec = {"super_steps": 0, "judged": 0, "rolled_back": 0, "worst_K": 0.0,
-           "worst_area": 0.0, "fp64_window_cells": 0}
+    per_block = STEPS * judge_every
+    blocks = n_steps // per_block
+    wins, bh, bw = _windows(plan, blocks, per_block, k, margin, halo) if blocks else ([], 1, 2)
+    ks = P.StepConst.from_buffer_copy(bytes(k))
+    ks.nx, ks.ny = bw, bh
+    fp64 = Solver(ks, Tm=Tm, device=dev, T0=k.Tamb) if blocks else None
+    diffs = torch.zeros(max(blocks, 1), dtype=torch.float64, device=dev)
+    areas = torch.zeros(max(blocks, 1), dtype=torch.float64, device=dev)
+    backs = torch.zeros(max(blocks, 1), dtype=torch.bool, device=dev)
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     x4 = torch.empty((k.ny, k.nx, 4), dtype=torch.bfloat16, device=dev)
-    for blk in range(blocks):
-        s_blk = blk * STEPS * judge_every
-        wy0, wy1, wx0, wx1 = _window(plan, s_blk, s_blk + STEPS * judge_every, k, margin,
-                                     k.nx, k.ny)
-        hy0, hy1 = max(0, wy0 - halo), min(k.ny, wy1 + halo)
-        hx0, hx1 = max(0, wx0 - halo), min(k.nx, wx1 + halo)
-        Tw0 = T[hy0:hy1, hx0:hx1].clone()
+    for blk, (wy0, wy1, wx0, wx1, oy, ox) in enumerate(wins):
+        s_blk = blk * per_block
+        fp64.set_field(T[oy:oy + bh, ox:ox + bw])
         for j in range(judge_every):
             s = s_blk + j * STEPS
             features(T, k, plan[s:s + STEPS], out=x4)
             y = net.forward(x4[None])
             apply(T, y[0])
-            rec["super_steps"] += 1
-        # FP64 judge on the window (halo cells give it the surroundings)
-        ks = P.StepConst.from_buffer_copy(bytes(k))
-        ks.nx, ks.ny = hx1 - hx0, hy1 - hy0
-        sub_plan = plan[s_blk:s_blk + STEPS * judge_every].copy()
-        sub_plan["x_l"] -= hx0 * k.dx
-        sub_plan["y_l"] -= hy0 * k.dy
-        fp64 = Solver(ks, Tm=Tm, device=dev, T0=Tw0.cpu().numpy())
+        # FP64 judge on the window (the box's other cells give it the surroundings)
+        sub_plan = plan[s_blk:s_blk + per_block].copy()
+        sub_plan["x_l"] -= ox * k.dx
+        sub_plan["y_l"] -= oy * k.dy
         fp64.advance(sub_plan)
-        iy0, iy1, ix0, ix1 = wy0 - hy0, wy1 - hy0, wx0 - hx0, wx1 - hx0
-        ref = fp64.field[iy0:iy1, ix0:ix1]
+        ref = fp64.field[wy0 - oy:wy1 - oy, wx0 - ox:wx1 - ox]
         got = T[wy0:wy1, wx0:wx1]
-        diff, area, back = judge(got, ref, tol_K, area_tol, Tm)
-        rec["judged"] += 1
-        rec["fp64_window_cells"] += (hy1 - hy0) * (hx1 - hx0)
-        rec["worst_K"] = max(rec["worst_K"], diff)
-        rec["worst_area"] = max(rec["worst_area"], area)
-        if back:
-            T[wy0:wy1, wx0:wx1] = ref
-            rec["rolled_back"] += 1
+        d, a, back = judge_device(got, ref, tol_K, area_tol, Tm)
+        diffs[blk], areas[blk], backs[blk] = d, a, back
+        got.copy_(torch.where(back, ref, got))
     e1.record()
     torch.cuda.synchronize(dev)
-    rec["gpu_ms"] = e0.elapsed_time(e1)
-    rec["steps"] = blocks * STEPS * judge_every
+    rb = backs[:blocks].cpu().numpy()
+    rec = {"super_steps": blocks * judge_every, "judged": blocks,
+           "rolled_back": int(rb.sum()),
+           "worst_K": float(diffs[:blocks].max().item()) if blocks else 0.0,
+           "worst_area": float(areas[:blocks].max().item()) if blocks else 0.0,
+           "fp64_window_cells": blocks * bh * bw, "judge_box": [bh, bw],
+           "gpu_ms": e0.elapsed_time(e1), "steps": blocks * per_block}
     return T, rec
 
 
