@@ -41,18 +41,25 @@ constexpr double INV_MUSHY = 1.0 / (T_LIQ - T_SOL);
 // points j-1 and j.  The reference evaluates the same chord as
 // y[j-1] + (T - t[j-1]) / (t[j] - t[j-1]) (y[j] - y[j-1]); the line form
 // agrees with it to a few ulp of y.  A cell's segment is the number of table
-// temperatures below T, counted on a 32-bit key of T (ext_key): for T >= 0
+// temperatures below T, decided on a 32-bit key of T (ext_key): for T >= 0
 // the key is twice the upper word of T's bit pattern plus one when the lower
 // word is non-zero, and every table temperature (an integer of at most 11
 // significant bits) has a zero lower word, so T > t_j exactly when
 // key(T) > key(t_j); a negative T gets key 0, segment 0, like the
-// reference's clamp, and a NaN the top segment.
+// reference's clamp, and a NaN the top segment.  The key's upper 16 bits
+// (exponent and 5 mantissa bits) cut [256, 2048) K into 96 buckets of
+// 8-32 K, none holding more than one table temperature (the closest two are
+// 60 K apart): a bucket's base segment (table temperatures below it) plus
+// one compare against the next table temperature gives the segment.
+constexpr int EXT_BUCKET0 = 0x407 << 5;   // upper 16 key bits of 256.0
+constexpr int EXT_BUCKETS = 96;           // up to 2048.0
 struct ExtLines {
     double ak[10], bk[10], ac[10], bc[10];
-    unsigned int tkey[9];              // keys of the table temperatures
+    unsigned int tkey[10];             // keys of the table temperatures; [9] = no bound
     unsigned int sol_key, liq_key;     // of T_SOL and T_LIQ
-    unsigned int pad;
+    unsigned char bseg[EXT_BUCKETS];   // base segment of each bucket
 };
+static_assert(sizeof(ExtLines) % sizeof(double) == 0, "copied to shared memory as doubles");
 
 inline unsigned int host_key(double v) {
     unsigned long long b;
@@ -74,9 +81,18 @@ ExtLines make_ext_lines() {
     L.ak[9] = EXT_K_PTS[8];  L.bk[9] = 0.0;
     L.ac[9] = EXT_CP_PTS[8]; L.bc[9] = 0.0;
     for (int j = 0; j < 9; ++j) L.tkey[j] = host_key(EXT_T_PTS[j]);
+    L.tkey[9] = 0xffffffffu;
     L.sol_key = host_key(T_SOL);
     L.liq_key = host_key(T_LIQ);
-    L.pad = 0;
+    for (int b = 0; b < EXT_BUCKETS; ++b) {
+        // the bucket's lowest value: upper word (EXT_BUCKET0 + b) << 15
+        const unsigned long long bits = (unsigned long long)(unsigned)(EXT_BUCKET0 + b) << 47;
+        double lo;
+        std::memcpy(&lo, &bits, sizeof(lo));
+        int base = 0;
+        while (base < 9 && EXT_T_PTS[base] < lo) ++base;
+        L.bseg[b] = (unsigned char)base;
+    }
     return L;
 }
 
@@ -161,13 +177,13 @@ __device__ __forceinline__ unsigned int ext_key(double T) {
     return (int)hi < 0 ? 0u : k;
 }
 
-// Segment of a key in the tables; the table keys are read from the kernel's
-// parameter space (the same for every lane).
-__device__ __forceinline__ int ext_seg(unsigned int key, const ExtLines& Lp) {
-    int s = 0;
-#pragma unroll
-    for (int j = 0; j < 9; ++j) s += (key > Lp.tkey[j]) ? 1 : 0;
-    return s;
+// Segment of a key in the tables (bucket base plus one compare; see
+// ExtLines), from the shared-memory copy of the tables.
+__device__ __forceinline__ int ext_seg(unsigned int key, const ExtLines& L) {
+    const int b = (int)(key >> 16) - EXT_BUCKET0;
+    const int base = L.bseg[min(max(b, 0), EXT_BUCKETS - 1)];
+    const int s = base + (key > L.tkey[base] ? 1 : 0);
+    return b < 0 ? 0 : (b >= EXT_BUCKETS ? 9 : s);
 }
 
 // k_eff(T) = k_of(T) k_enh(T, kmult) (params.hpp:91-105); kp = k_of(T).
@@ -196,7 +212,7 @@ __device__ __forceinline__ ExtCell ext_cell(double T, const ExtLines& L, const E
     ExtCell c;
     c.T = T;
     c.key = ext_key(T);
-    c.seg = ext_seg(c.key, Lp);
+    c.seg = ext_seg(c.key, L);
     c.k = ext_keff<KM>(T, c.key, c.seg, L, Lp, kmult, c.kp);
     return c;
 }

@@ -130,13 +130,26 @@ __device__ __forceinline__ void tmem_ld32(uint32_t addr, float* v) {
 
 // ---- activation ---------------------------------------------------------------
 
+// GELU in its tanh form (Hendrycks and Gimpel, "Gaussian Error Linear
+// Units", 2016): gelu(x) = x/2 (1 + tanh(u)), u = sqrt(2/pi) (x + 0.044715
+// x^3), and its derivative.  tanh is the hardware's tanh.approx.f32 (about
+// 11 significant bits): the activations it feeds are stored in bf16 (8).
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float GELU_C = 0.7978845608028654f;      // sqrt(2 / pi)
+constexpr float GELU_A = 0.044715f;
 __device__ __forceinline__ float gelu(float x) {
-    return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f));
+    const float u = GELU_C * fmaf(GELU_A * x, x * x, x);
+    return 0.5f * x * (1.0f + tanh_approx(u));
 }
 __device__ __forceinline__ float gelu_grad(float x) {
-    const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
-    const float pdf = 0.39894228040143268f * expf(-0.5f * x * x);
-    return cdf + x * pdf;
+    const float x2 = x * x;
+    const float t = tanh_approx(GELU_C * fmaf(GELU_A * x, x2, x));
+    const float du = GELU_C * fmaf(3.0f * GELU_A, x2, 1.0f);
+    return 0.5f * (1.0f + t) + 0.5f * x * fmaf(-t, t, 1.0f) * du;
 }
 
 }  // namespace sg

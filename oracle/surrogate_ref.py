@@ -12,7 +12,6 @@ from __future__ import annotations
 import math
 
 import numpy as np
-from scipy.special import erf
 
 TAPS = [(t // 3 - 1, t % 3 - 1) for t in range(9)]
 CH = (4, 32, 32, 32, 32, 1)          # channels of the 5 layers' inputs/outputs
@@ -62,12 +61,17 @@ def pack(w: np.ndarray, n_pad: int | None = None, k_pad: int | None = None) -> n
     return out
 
 
+GELU_C, GELU_A = math.sqrt(2.0 / math.pi), 0.044715
+
+
 def gelu(x):
-    return 0.5 * x * (1.0 + erf(x / math.sqrt(2.0)))
+    """GELU, tanh form (Hendrycks and Gimpel 2016), as the kernels use it."""
+    return 0.5 * x * (1.0 + np.tanh(GELU_C * (x + GELU_A * x ** 3)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2 * math.pi)
+    t = np.tanh(GELU_C * (x + GELU_A * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * GELU_C * (1.0 + 3.0 * GELU_A * x * x)
 
 
 def init_params(seed: int = 0):
