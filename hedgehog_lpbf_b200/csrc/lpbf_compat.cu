@@ -125,7 +125,7 @@ constexpr int EXT_WARPS = 8;       // warps per CTA
 constexpr int EXT_V = 2;           // columns per lane
 constexpr int EXT_OWN = 32 * EXT_V - 2;   // columns a warp owns (the first and last are halo)
 constexpr int EXT_H = 64;          // rows per task
-constexpr int EXT_PF = 4;          // rows loaded ahead of the one being updated
+constexpr int EXT_PF = 8;          // rows loaded ahead of the one being updated
 
 struct ExtParams {
     StepConst k;

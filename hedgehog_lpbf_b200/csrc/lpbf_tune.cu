@@ -8,7 +8,10 @@
 // are chosen by timing short runs of the batch kernel, with CUDA events, on
 // a subset of the caller's scenarios (their own grids and plans, fields
 // filled with T_amb in scratch memory the tuner allocates and frees):
-//   1. per size class present, rows in {12, 24, 48, 96, 192} at depth 3;
+//   1. per size class present, rows in {12, 24, 48, 96, 192, 384}, timed on
+//      all classes' subsets together (the classes share the launches, so a
+//      class's best rows depend on the others' work beside it), one class
+//      after another from (24, 48, 96, 192) at depth 2;
 //   2. on all subsets together, depth in {2, 3, 4} x CTAs per SM in
 //      {all, all - 1} x staging in {bulk, maps}, with the rows of step 1.
 // The winner is stored in a JSON file under a key made of the GPU's name,
@@ -341,22 +344,26 @@ int lpbf_b200_batch_autotune(const lpbf_b200_scenario* sc, int n_scen, int n_ste
     }
     if (cudaStreamSynchronize(s) != cudaSuccess) { cudaStreamDestroy(s); return LPBF_ERR_CUDA; }
 
+    std::vector<lpbf_b200_scenario> all;
+    for (int c = 0; c < 4; ++c) all.insert(all.end(), by_class[c].begin(), by_class[c].end());
     lpbf_b200_batch_opts best;
     std::memset(&best, 0, sizeof(best));
-    best.depth = 3;
-    static const int ROWS[] = {12, 24, 48, 96, 192};
+    best.depth = 2;
+    static const int START[4] = {24, 48, 96, 192};
+    for (int c = 0; c < 4; ++c) best.rows[c] = START[c];
+    static const int ROWS[] = {12, 24, 48, 96, 192, 384};
     for (int c = 0; c < 4; ++c) {
         if (by_class[c].empty()) continue;
         double bg = 0.0;
+        int br = best.rows[c];
         for (int r : ROWS) {
             lpbf_b200_batch_opts o = best;
             o.rows[c] = r;
-            const double g = trial(by_class[c], trial_steps, o, s);
-            if (g > bg) { bg = g; best.rows[c] = r; }
+            const double g = trial(all, trial_steps, o, s);
+            if (g > bg) { bg = g; br = r; }
         }
+        best.rows[c] = br;
     }
-    std::vector<lpbf_b200_scenario> all;
-    for (int c = 0; c < 4; ++c) all.insert(all.end(), by_class[c].begin(), by_class[c].end());
     double bg = 0.0;
     lpbf_b200_batch_opts win = best;
     for (int d : {2, 3, 4}) {
