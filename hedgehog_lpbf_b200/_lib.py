@@ -120,6 +120,8 @@ SIGNATURES = {
                                                 ctypes.c_double]),
     "lpbf_b200_sg_conv": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(SgConvArgs), _vp]),
     "lpbf_b200_sg_gemm_bt": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "lpbf_b200_sg_set_form": (ctypes.c_int, [ctypes.c_int]),
+    "lpbf_b200_sg_form_used": (ctypes.c_int, []),
     "lpbf_b200_sg_param_count": (ctypes.c_int, []),
     "lpbf_b200_sg_net_bytes": (ctypes.c_size_t, []),
     "lpbf_b200_sg_work_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int, ctypes.c_int,

@@ -118,6 +118,26 @@ bool tensor_map_act_bf16(const void* base, int C, int W, int H, int B, int box_p
            CUDA_SUCCESS;
 }
 
+// NHWC bf16 activations with 4 channels (8 bytes per pixel) as a 4D tensor
+// of pixel pairs (8 values, W / 2 pairs, H, B; W even): a box {8, box_pairs,
+// 1, 1} brings 2 box_pairs consecutive pixels of one row, unswizzled (a TMA
+// box row must hold a multiple of 16 bytes).  Pixels and rows off the image
+// read as zero.
+bool tensor_map_pixel_pairs_bf16(const void* base, int W, int H, int B, int box_pairs,
+                                 CUtensorMap* out) {
+    EncodeFn fn = encode_fn();
+    if (!fn || W % 2 != 0 || box_pairs < 1 || box_pairs > 256) return false;
+    cuuint64_t gdim[4] = {8, (cuuint64_t)W / 2, (cuuint64_t)H, (cuuint64_t)B};
+    cuuint64_t gstride[3] = {16, (cuuint64_t)8 * W, (cuuint64_t)8 * W * H};
+    cuuint32_t box[4] = {8, (cuuint32_t)box_pairs, 1, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    std::memset(out, 0, sizeof(*out));
+    return fn(out, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), gdim, gstride,
+              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+}
+
 // ---- launch of one temporally blocked step ---------------------------------
 namespace {
 

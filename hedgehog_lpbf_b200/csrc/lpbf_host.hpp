@@ -50,6 +50,8 @@ bool tensor_map_f64(const void* base, int nx, int ny, int box_cols, int box_rows
                     CUtensorMap* out);
 bool tensor_map_f32(const void* base, int nx, int ny, int box_cols, int box_rows,
                     CUtensorMap* out);
+bool tensor_map_pixel_pairs_bf16(const void* base, int W, int H, int B, int box_pairs,
+                                 CUtensorMap* out);
 bool tensor_map_act_bf16(const void* base, int C, int W, int H, int B, int box_px,
                          CUtensorMap* out);
 

@@ -28,6 +28,12 @@ namespace sg {
 
 enum { EPI_GELU = 0, EPI_LINEAR = 1, EPI_DGELU = 2 };
 
+// Form of the 32-channel layers and of the input layer (LPBF_SG_FORM_*):
+// row-streaming, tap-tile (32-channel layers only) or plain; each form falls
+// back to the next when it cannot run.
+int g_conv_form = 0;
+int g_conv_form_used = -1;          // form of the last FWD_IN or 32-channel launch
+
 struct ConvArgs {
     const void* x;          // input, NHWC bf16 with CIN channels
     const bf16* w;          // [N][K] packed weights
@@ -294,6 +300,47 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
 }
 
+// Epilogue of 16 accumulator columns (channels c0 .. c0 + 15) of pixel p.
+// GELU: bias, pre-activation and activation out (bf16); LINEAR: channel 0
+// plus bias (fp32); DGELU: times gelu'(pre_in) (bf16).
+template <int N, int EPI>
+__device__ __forceinline__ void epilogue16(const ConvArgs& a, size_t p, int c0, const float* v,
+                                           const float* bias) {
+    if constexpr (EPI == EPI_LINEAR) {
+        static_cast<float*>(a.out)[p] = v[0] + (a.bias ? a.bias[0] : 0.0f);
+    } else {
+        uint32_t o[8], pr[8];
+        if constexpr (EPI == EPI_GELU) {
+#pragma unroll
+            for (int c = 0; c < 16; c += 2) {
+                const float v0 = v[c] + bias[c], v1 = v[c + 1] + bias[c + 1];
+                pr[c / 2] = pack_bf16(v0, v1);
+                o[c / 2] = pack_bf16(gelu(v0), gelu(v1));
+            }
+        } else {
+            const uint4* src = reinterpret_cast<const uint4*>(a.pre_in + p * N + c0);
+            const uint4 u0 = __ldg(src), u1 = __ldg(src + 1);
+            const uint32_t w[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+#pragma unroll
+            for (int c = 0; c < 16; c += 2) {
+                const float g0 = __uint_as_float(w[c / 2] << 16);
+                const float g1 = __uint_as_float(w[c / 2] & 0xffff0000u);
+                o[c / 2] = pack_bf16(v[c] * gelu_grad(g0), v[c + 1] * gelu_grad(g1));
+            }
+        }
+        uint4* dst = reinterpret_cast<uint4*>(static_cast<bf16*>(a.out) + p * N + c0);
+        dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+        dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+        if constexpr (EPI == EPI_GELU) {
+            if (a.pre_out) {
+                uint4* dp = reinterpret_cast<uint4*>(a.pre_out + p * N + c0);
+                dp[0] = make_uint4(pr[0], pr[1], pr[2], pr[3]);
+                dp[1] = make_uint4(pr[4], pr[5], pr[6], pr[7]);
+            }
+        }
+    }
+}
+
 template <int N>
 constexpr size_t ct_smem_bytes() {
     return 1024 + size_t(CT_STAGES) * CT_STAGE_BYTES + size_t(N) * 288 * 2;
@@ -381,43 +428,325 @@ conv_tma_kernel(const __grid_constant__ CUtensorMap xmap, const ConvArgs a, int 
             const int y = row % a.H, b = row / a.H;
             const int x = xt * 128 + q * 32 + lane;
             if (!active || x >= a.W) continue;
-            const size_t p = (size_t(b) * a.H + y) * a.W + x;
-            const int c0 = 16 * h;
-            if constexpr (EPI == EPI_LINEAR) {
-                static_cast<float*>(a.out)[p] = v[0] + (a.bias ? a.bias[0] : 0.0f);
-            } else {
-                uint32_t o[8], pr[8];
-#pragma unroll
-                for (int c = 0; c < 16; c += 2) {
-                    float v0 = v[c], v1 = v[c + 1];
-                    if constexpr (EPI == EPI_GELU) {
-                        v0 += bias[c];
-                        v1 += bias[c + 1];
-                        pr[c / 2] = pack_bf16(v0, v1);
-                        o[c / 2] = pack_bf16(gelu(v0), gelu(v1));
-                    } else {
-                        const float g0 = gelu_grad(bf16_at(a.pre_in, p * N + c0 + c));
-                        const float g1 = gelu_grad(bf16_at(a.pre_in, p * N + c0 + c + 1));
-                        o[c / 2] = pack_bf16(v0 * g0, v1 * g1);
-                    }
-                }
-                uint4* dst = reinterpret_cast<uint4*>(static_cast<bf16*>(a.out) + p * N + c0);
-                dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
-                dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
-                if constexpr (EPI == EPI_GELU) {
-                    if (a.pre_out) {
-                        uint4* dp = reinterpret_cast<uint4*>(a.pre_out + p * N + c0);
-                        dp[0] = make_uint4(pr[0], pr[1], pr[2], pr[3]);
-                        dp[1] = make_uint4(pr[4], pr[5], pr[6], pr[7]);
-                    }
-                }
-            }
+            epilogue16<N, EPI>(a, (size_t(b) * a.H + y) * a.W + x, 16 * h, v, bias);
         }
     }
     if (!ok && a.err) atomicOr(a.err, 1u);
     tc_fence_before();
     __syncthreads();
     if (warp == 1) tmem_free(tmem, 2 * ACC_COLS);
+}
+
+// ---- row-streaming form (32- and 4-channel inputs) --------------------------
+//
+// A CTA walks runs of CR_RUN output rows of one 128-pixel column tile, three
+// CTAs per SM.  Warp 0 streams the run's input rows, plus one above and one
+// below, by TMA into a ring of slots; each input row crosses from L2 once
+// per run instead of once per tap.
+//   32 channels: a slot holds 130 pixels (the tile and one either side) of
+//     one row, 64 bytes each, with the 64-byte swizzle, which is the tensor
+//     core's K-major SW64 operand layout.  The A operand of tap (dy, dx) is
+//     the slot of input row y + dy - 1 from its pixel dx on: the start
+//     address moves by 64 bytes per pixel (the swizzle follows the address
+//     bits, so the shifted operand reads what TMA wrote), no im2col copy.
+//     18 MMAs per output row (9 taps x 2 halves of 16 channels).
+//   4 channels: TMA brings 132 pixels of a row (8 bytes each, as pixel
+//     pairs: a TMA box row must be a multiple of 16 bytes) into a small raw
+//     ring; the 32 lanes of warp 0 then write the row's three x-taps per
+//     pixel, (x-1, x, x+1) x 4 channels plus 4 zeros, as a K = 16 no-swizzle
+//     operand slot.  An output row is then 3 MMAs, one per input row dy.
+// Warp 1 issues an output row's MMAs into one of two TMEM accumulators,
+// releases the input slot that no later output of the run reads (all three
+// after the run's last output) and commits to the accumulator's "full"
+// barrier; warps 2-9 run the epilogue as in the tap-tile form.  Waits are
+// bounded; after a timeout the CTA records the error, waits (bounded) for
+// its copies and MMAs in flight, frees its TMEM and returns.
+constexpr int CR_PX = 130;                         // pixels of a 32-channel slot
+constexpr int CR_ROW_BYTES = CR_PX * 64;           // 8320 bytes loaded per row
+constexpr int CR_PITCH32 = 8704;                   // slot pitch: 512-byte swizzle period
+constexpr int CR_X3_BYTES = 2 * 128 * 16;          // 4-channel operand slot
+constexpr int CR_RAW_PAIRS = 66;                   // 132 pixels of a 4-channel row
+constexpr int CR_RAW_BYTES = CR_RAW_PAIRS * 16;   // loaded per 4-channel row
+constexpr int CR_RAW_PITCH = 1152;                 // raw slot pitch
+constexpr int CR_RAW = 4;                          // raw 4-channel row slots
+constexpr int CR_SLOTS = 5;                        // operand slots
+constexpr int CR_RUN = 32;                         // output rows per work unit
+constexpr int CR_CTAS = 3;                         // CTAs per SM
+constexpr int CR_NACC = 2;                         // TMEM accumulators
+// a TMA tensor copy lands on a 128-byte boundary
+static_assert(CR_PITCH32 % 512 == 0 && CR_X3_BYTES % 128 == 0 && CR_RAW_PITCH % 128 == 0 &&
+                  CR_RAW_PITCH >= CR_RAW_BYTES && CR_PITCH32 >= CR_ROW_BYTES,
+              "row slots");
+
+template <int CIN, int N>
+constexpr size_t cr_smem_bytes() {
+    return CIN == 32 ? 1024 + size_t(CR_SLOTS) * CR_PITCH32 + size_t(N) * 288 * 2
+                     : 1024 + size_t(CR_SLOTS) * CR_X3_BYTES + size_t(CR_RAW) * CR_RAW_PITCH +
+                           3 * size_t(N) * 32;
+}
+
+// Work unit u: column tile xt, image b, output rows y0 .. y0 + n - 1.
+struct RowUnit { int b, xt, y0, n; };
+__device__ __forceinline__ RowUnit row_unit(int u, int xtiles, int runs, int H) {
+    RowUnit r;
+    r.xt = u % xtiles;
+    const int t = u / xtiles;
+    r.b = t / runs;
+    r.y0 = (t % runs) * CR_RUN;
+    r.n = min(CR_RUN, H - r.y0);
+    return r;
+}
+
+// The input rows of a CTA's units in order: unit u, row L = 0 .. n + 1
+// (field row y0 - 1 + L).
+struct RowCursor {
+    int u, L, nunits, xtiles, runs, H;
+    RowUnit r;
+    __device__ RowCursor(int u0, int nu, int xt, int ru, int h)
+        : u(u0), L(0), nunits(nu), xtiles(xt), runs(ru), H(h) {
+        if (u < nunits) r = row_unit(u, xtiles, runs, H);
+    }
+    __device__ bool valid() const { return u < nunits; }
+    __device__ void next() {
+        if (++L == r.n + 2) {
+            L = 0;
+            u += gridDim.x;
+            if (u < nunits) r = row_unit(u, xtiles, runs, H);
+        }
+    }
+};
+
+// No-swizzle K-major operand layouts in bf16 elements, (rows, K = 16) of one
+// MMA: rows 16 bytes apart in groups of 8 (128 bytes), the two 8-entry
+// halves of K 128 rows (A, 4-channel slot) or N rows (weights) apart.
+using LayX3 = cute::Layout<cute::Shape<cute::Shape<cute::_8, cute::_16>,
+                                       cute::Shape<cute::_8, cute::_2>>,
+                           cute::Stride<cute::Stride<cute::_8, cute::_64>,
+                                        cute::Stride<cute::_1, cute::_1024>>>;
+template <int N>
+using LayRowB = cute::Layout<cute::Shape<cute::Shape<cute::_8, cute::Int<N / 8>>,
+                                         cute::Shape<cute::_8, cute::_2>>,
+                             cute::Stride<cute::Stride<cute::_8, cute::_64>,
+                                          cute::Stride<cute::_1, cute::Int<N * 8>>>>;
+
+template <int CIN, int N, int EPI>
+__global__ void __launch_bounds__(CT_THREADS, CR_CTAS)
+conv_row_kernel(const __grid_constant__ CUtensorMap xmap, const ConvArgs a, int nunits,
+                int xtiles, int runs) {
+    static_assert(CIN == 32 || (CIN == 4 && N == 32), "row-streaming layers");
+    using Mma = cute::SM100_MMA_F16BF16_SS<bf16, bf16, float, 128, N, cute::UMMA::Major::K,
+                                           cute::UMMA::Major::K>;
+    constexpr int ACC_COLS = N < 32 ? 32 : N;
+    constexpr uint32_t S = CR_SLOTS;
+    constexpr int PITCH = CIN == 32 ? CR_PITCH32 : CR_X3_BYTES;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ uint64_t full[CR_SLOTS], empty[CR_SLOTS], rfull[CR_RAW], tfull[CR_NACC],
+        tempty[CR_NACC], drain;
+    __shared__ uint32_t tslot;
+    uint8_t* base = align1024(smem_raw);
+    uint8_t* sRows = base;                           // operand slots
+    uint8_t* sRaw = base + size_t(CR_SLOTS) * PITCH; // 4-channel raw rows
+    uint8_t* sB = CIN == 32 ? sRaw : sRaw + size_t(CR_RAW) * CR_RAW_PITCH;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (warp == 1) tmem_alloc(&tslot, CR_NACC * ACC_COLS);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < CR_SLOTS; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
+        for (int i = 0; i < CR_RAW; ++i) mbar_init(&rfull[i], 1);
+        for (int i = 0; i < CR_NACC; ++i) {
+            mbar_init(&tfull[i], 1);
+            mbar_init(&tempty[i], CT_EPI_WARPS);
+        }
+        mbar_init(&drain, 1);
+        fence_mbar_init();
+    }
+    if constexpr (CIN == 32) {
+        // weights, K-major without swizzle: the 16-byte unit of output
+        // channel n and input entries k .. k + 7 at (k / 8) * N * 16 + n * 16
+        for (int u = threadIdx.x; u < N * 36; u += blockDim.x) {
+            const int n = u % N, kc = u / N;
+            *reinterpret_cast<uint4*>(sB + size_t(kc) * N * 16 + n * 16) =
+                __ldg(reinterpret_cast<const uint4*>(a.w + size_t(n) * 288 + kc * 8));
+        }
+    } else {
+        // one K = 16 weight tile per input row dy: entry k' = dx * 4 + ci is
+        // packed entry (3 dy + dx) * 4 + ci = 12 dy + k' of [N][64]; 12..15 zero
+        uint16_t* B16 = reinterpret_cast<uint16_t*>(sB);
+        const uint16_t* w16 = reinterpret_cast<const uint16_t*>(a.w);
+        for (int e = threadIdx.x; e < 3 * N * 16; e += blockDim.x) {
+            const int kk = e & 15, n = (e >> 4) % N, dy = e / (16 * N);
+            B16[(dy * 2 * N * 16 + (kk >> 3) * N * 16 + n * 16) / 2 + (kk & 7)] =
+                kk < 12 ? w16[n * 64 + 12 * dy + kk] : uint16_t(0);
+        }
+    }
+    fence_smem_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tslot;
+    bool ok = true;
+
+    if (warp == 0) {
+        if constexpr (CIN == 32) {
+            if (lane == 0) {
+                uint32_t g = 0;                      // input rows issued
+                for (RowCursor c(blockIdx.x, nunits, xtiles, runs, a.H); c.valid(); c.next(), ++g) {
+                    const uint32_t s = g % S;
+                    if (!mbar_wait_bounded(&empty[s], ((g / S) & 1) ^ 1)) { ok = false; break; }
+                    mbar_expect_tx(&full[s], CR_ROW_BYTES);
+                    tma_load_4d(sRows + size_t(s) * PITCH, &xmap, 0, c.r.xt * 128 - 1,
+                                c.r.y0 - 1 + c.L, c.r.b, &full[s]);
+                }
+                // the last copy issued into each slot has landed
+                for (uint32_t i = 0; i < S && i < g; ++i) {
+                    const uint32_t gi = g - 1 - i;
+                    if (!mbar_wait_bounded(&full[gi % S], (gi / S) & 1)) ok = false;
+                }
+            }
+        } else {
+            RowCursor c(blockIdx.x, nunits, xtiles, runs, a.H);
+            uint32_t issued = 0, g = 0;
+            auto issue = [&]() {                     // next raw row into its slot
+                if (lane == 0) {
+                    const uint32_t rs = issued % CR_RAW;
+                    fence_smem_async();              // earlier reads of the slot first
+                    mbar_expect_tx(&rfull[rs], CR_RAW_BYTES);
+                    tma_load_4d(sRaw + size_t(rs) * CR_RAW_PITCH, &xmap, 0,
+                                c.r.xt * 64 - 1, c.r.y0 - 1 + c.L, c.r.b, &rfull[rs]);
+                }
+                ++issued;
+                c.next();
+            };
+            for (int i = 0; i < CR_RAW && c.valid(); ++i) issue();
+            for (; g < issued; ++g) {
+                const uint32_t rs = g % CR_RAW, s = g % S;
+                bool w = mbar_wait_bounded(&rfull[rs], (g / CR_RAW) & 1);
+                w = w && mbar_wait_bounded(&empty[s], ((g / S) & 1) ^ 1);
+                if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
+                // raw pixel i is field pixel xt * 128 - 2 + i; slot row m takes
+                // pixels m - 1, m (first half of K) and m + 1 (second half)
+                const uint8_t* rp = sRaw + size_t(rs) * CR_RAW_PITCH;
+                uint8_t* xp = sRows + size_t(s) * PITCH;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int m = lane + 32 * i;
+                    const uint2 p0 = *reinterpret_cast<const uint2*>(rp + (m + 1) * 8);
+                    const uint2 p1 = *reinterpret_cast<const uint2*>(rp + (m + 2) * 8);
+                    const uint2 p2 = *reinterpret_cast<const uint2*>(rp + (m + 3) * 8);
+                    *reinterpret_cast<uint4*>(xp + m * 16) = make_uint4(p0.x, p0.y, p1.x, p1.y);
+                    *reinterpret_cast<uint4*>(xp + 2048 + m * 16) = make_uint4(p2.x, p2.y, 0u, 0u);
+                }
+                fence_smem_async();                  // visible to the tensor core
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&full[s]);
+                if (c.valid()) issue();
+            }
+            // copies issued and not consumed have landed
+            for (uint32_t gi = g; gi < issued; ++gi)
+                if (!mbar_wait_bounded(&rfull[gi % CR_RAW], (gi / CR_RAW) & 1)) ok = false;
+        }
+    } else if (warp == 1) {
+        using namespace cute;
+        const uint64_t idesc =
+            UMMA::make_runtime_instr_desc<bf16, bf16, float, 128, N, UMMA::Major::K,
+                                          UMMA::Major::K>();
+        uint64_t dA0;
+        if constexpr (CIN == 32) {
+            // K-major, 64-byte swizzle: rows 64 bytes apart, 8-row groups 512
+            UMMA::SmemDescriptor d;
+            d.version_ = 1;
+            d.lbo_mode_ = 0;
+            d.layout_type_ = uint8_t(UMMA::LayoutType::SWIZZLE_64B);
+            d.start_address_ = uint16_t(smem_u32(sRows) >> 4);
+            d.base_offset_ = 0;
+            d.leading_byte_offset_ = 1;
+            d.stride_byte_offset_ = 512 >> 4;
+            dA0 = d;
+        } else {
+            dA0 = UMMA::make_umma_desc<UMMA::Major::K>(
+                make_tensor(make_smem_ptr(reinterpret_cast<bf16*>(sRows)), LayX3{}));
+        }
+        const uint64_t dB0 = UMMA::make_umma_desc<UMMA::Major::K>(
+            make_tensor(make_smem_ptr(reinterpret_cast<bf16*>(sB)), LayRowB<N>{}));
+        uint32_t g = 0, o = 0;                       // first input row of the unit; outputs
+        for (int u = blockIdx.x; ok && u < nunits; u += gridDim.x) {
+            const RowUnit r = row_unit(u, xtiles, runs, a.H);
+            for (int j = 0; j < r.n; ++j, ++o) {
+                const int acc = o % CR_NACC;
+                bool w = mbar_wait_bounded(&tempty[acc], ((o / CR_NACC) & 1) ^ 1);
+#pragma unroll
+                for (int dy = 0; dy < 3; ++dy) {
+                    const uint32_t gi = g + j + dy;
+                    w = w && mbar_wait_bounded(&full[gi % S], (gi / S) & 1);
+                }
+                if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
+                tc_fence_after();
+                const uint32_t d = tmem + acc * ACC_COLS;
+#pragma unroll
+                for (int dy = 0; dy < 3; ++dy) {
+                    // start addresses in 16-byte units
+                    const uint64_t da = dA0 + ((g + j + dy) % S) * (PITCH >> 4);
+                    if constexpr (CIN == 32) {
+#pragma unroll
+                        for (int dx = 0; dx < 3; ++dx) {
+#pragma unroll
+                            for (int h = 0; h < 2; ++h) {
+                                const int tap = dy * 3 + dx;
+                                Mma::fma(da + 4 * dx + 2 * h, dB0 + (tap * 4 + 2 * h) * N, d,
+                                         (tap | h) != 0 ? 1u : 0u, idesc);
+                            }
+                        }
+                    } else {
+                        Mma::fma(da, dB0 + dy * 2 * N, d, dy != 0 ? 1u : 0u, idesc);
+                    }
+                }
+                cutlass::arch::umma_arrive(&empty[(g + j) % S]);
+                if (j == r.n - 1) {
+                    cutlass::arch::umma_arrive(&empty[(g + j + 1) % S]);
+                    cutlass::arch::umma_arrive(&empty[(g + j + 2) % S]);
+                }
+                cutlass::arch::umma_arrive(&tfull[acc]);
+            }
+            g += r.n + 2;
+        }
+        // every MMA issued has completed before the accumulators are freed
+        cutlass::arch::umma_arrive(&drain);
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&drain, 0))) ok = false;
+    } else {
+        const int q = warp & 3;                      // TMEM lane quarter of this warp
+        const int h = (warp - 2) >> 2;               // column half: 0 or 1
+        const bool active = N == 32 || h == 0;
+        float bias[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c)
+            bias[c] = (EPI == EPI_GELU && active) ? __ldg(a.bias + 16 * h + c) : 0.0f;
+        uint32_t o = 0;
+        for (int u = blockIdx.x; ok && u < nunits; u += gridDim.x) {
+            const RowUnit r = row_unit(u, xtiles, runs, a.H);
+            for (int j = 0; j < r.n; ++j, ++o) {
+                const int acc = o % CR_NACC;
+                if (!__all_sync(0xffffffffu,
+                                mbar_wait_bounded(&tfull[acc], (o / CR_NACC) & 1))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                float v[16];
+                if (active)
+                    tmem_ld16(tmem + acc * ACC_COLS + (uint32_t(q * 32) << 16) + 16 * h, v);
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[acc]);
+                const int x = r.xt * 128 + q * 32 + lane;
+                if (!active || x >= a.W) continue;
+                epilogue16<N, EPI>(a, (size_t(r.b) * a.H + r.y0 + j) * a.W + x, 16 * h, v, bias);
+            }
+        }
+    }
+    if (!ok && a.err) atomicOr(a.err, 1u);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) tmem_free(tmem, CR_NACC * ACC_COLS);
 }
 
 template <int N, int EPI>
@@ -444,6 +773,32 @@ cudaError_t launch_conv_tma(const ConvArgs& a, cudaStream_t s) {
 }
 
 template <int CIN, int N, int EPI>
+cudaError_t launch_conv_row(const ConvArgs& a, cudaStream_t s) {
+    CUtensorMap map;
+    if (reinterpret_cast<uintptr_t>(a.x) % 16 != 0) return cudaErrorNotSupported;
+    if (CIN == 32 ? !tensor_map_act_bf16(a.x, 32, a.W, a.H, a.B, CR_PX, &map)
+                  : (a.W % 2 != 0 || !tensor_map_pixel_pairs_bf16(a.x, a.W, a.H, a.B,
+                                                                   CR_RAW_PAIRS, &map)))
+        return cudaErrorNotSupported;
+    constexpr size_t smem = cr_smem_bytes<CIN, N>();
+    auto kern = conv_row_kernel<CIN, N, EPI>;
+    static bool attr = false;
+    if (!attr) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const int xtiles = (a.W + 127) / 128;
+    const int runs = (a.H + CR_RUN - 1) / CR_RUN;
+    const long long nu = (long long)xtiles * runs * a.B;
+    if (nu >= (1ll << 31)) return cudaErrorInvalidValue;
+    const int grid = (int)std::min<long long>(nu, (long long)CR_CTAS * sm_count());
+    kern<<<grid, CT_THREADS, smem, s>>>(map, a, (int)nu, xtiles, runs);
+    return cudaGetLastError();
+}
+
+template <int CIN, int N, int EPI>
 cudaError_t launch_conv(const ConvArgs& a, cudaStream_t s) {
     constexpr size_t smem = conv_smem_bytes<CIN, N>();
     auto kern = conv_kernel<CIN, N, EPI>;
@@ -457,6 +812,23 @@ cudaError_t launch_conv(const ConvArgs& a, cudaStream_t s) {
     const dim3 grid((a.W + 127) / 128, a.H, a.B);
     kern<<<grid, 128, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+// Row-streaming form first, then the tap-tile form, then the plain one (each
+// declines with cudaErrorNotSupported when its tensor map cannot be made).
+template <int N, int EPI>
+cudaError_t launch_conv32(const ConvArgs& a, cudaStream_t s) {
+    g_conv_form_used = 0;
+    cudaError_t e = g_conv_form == 0 ? launch_conv_row<32, N, EPI>(a, s) : cudaErrorNotSupported;
+    if (e == cudaErrorNotSupported && g_conv_form <= 1) {
+        g_conv_form_used = 1;
+        e = launch_conv_tma<N, EPI>(a, s);
+    }
+    if (e == cudaErrorNotSupported) {
+        g_conv_form_used = 2;
+        e = launch_conv<32, N, EPI>(a, s);
+    }
+    return e;
 }
 
 }  // namespace sg
@@ -486,29 +858,38 @@ int lpbf_b200_sg_conv(int kind, const lpbf_b200_sg_conv_args* p, cudaStream_t st
     switch (kind) {
         case LPBF_SG_FWD_IN:
             if (!a.bias) return LPBF_ERR_ARG;
-            e = launch_conv<4, 32, EPI_GELU>(a, stream); break;
+            g_conv_form_used = 0;
+            e = g_conv_form == 0 ? launch_conv_row<4, 32, EPI_GELU>(a, stream)
+                                 : cudaErrorNotSupported;
+            if (e == cudaErrorNotSupported) {
+                g_conv_form_used = 2;
+                e = launch_conv<4, 32, EPI_GELU>(a, stream);
+            }
+            break;
         case LPBF_SG_FWD_HIDDEN:
             if (!a.bias) return LPBF_ERR_ARG;
-            e = launch_conv_tma<32, EPI_GELU>(a, stream);
-            if (e == cudaErrorNotSupported) e = launch_conv<32, 32, EPI_GELU>(a, stream);
-            break;
+            e = launch_conv32<32, EPI_GELU>(a, stream); break;
         case LPBF_SG_FWD_OUT:
-            e = launch_conv_tma<16, EPI_LINEAR>(a, stream);
-            if (e == cudaErrorNotSupported) e = launch_conv<32, 16, EPI_LINEAR>(a, stream);
-            break;
+            e = launch_conv32<16, EPI_LINEAR>(a, stream); break;
         case LPBF_SG_DX_OUT:
             if (!a.pre_in) return LPBF_ERR_ARG;
             e = launch_conv<1, 32, EPI_DGELU>(a, stream); break;
         case LPBF_SG_DX_HIDDEN:
             if (!a.pre_in) return LPBF_ERR_ARG;
-            e = launch_conv_tma<32, EPI_DGELU>(a, stream);
-            if (e == cudaErrorNotSupported) e = launch_conv<32, 32, EPI_DGELU>(a, stream);
-            break;
+            e = launch_conv32<32, EPI_DGELU>(a, stream); break;
         default:
             return LPBF_ERR_ARG;
     }
     return e == cudaSuccess ? LPBF_OK : LPBF_ERR_CUDA;
 }
+
+int lpbf_b200_sg_set_form(int form) {
+    if (form < LPBF_SG_FORM_ROWS || form > LPBF_SG_FORM_PLAIN) return LPBF_ERR_ARG;
+    g_conv_form = form;
+    return LPBF_OK;
+}
+
+int lpbf_b200_sg_form_used(void) { return g_conv_form_used; }
 
 int lpbf_b200_sg_gemm_bt(const void* A, const void* B, float* C, int n, int k, unsigned int* err,
                          cudaStream_t stream) {

@@ -309,6 +309,23 @@ typedef struct lpbf_b200_sg_conv_args {
     unsigned int* err;
 } lpbf_b200_sg_conv_args;
 int lpbf_b200_sg_conv(int kind, const lpbf_b200_sg_conv_args* args, cudaStream_t stream);
+/* Kernel form of the 32-channel kinds (FWD_HIDDEN, FWD_OUT, DX_HIDDEN) and
+ * of FWD_IN for this process, default LPBF_SG_FORM_ROWS:
+ *   ROWS   input rows streamed by TMA once per run of output rows; 32
+ *          channels: taps as pixel-shifted tensor-core operands; FWD_IN
+ *          (even widths): each row's three x-taps written once, three MMAs
+ *          per output row;
+ *   TILES  32-channel kinds: nine TMA tap tiles per 128-pixel tile;
+ *   PLAIN  im2col tile gathered by all threads.
+ * A form that cannot run (its tensor map cannot be encoded, an odd FWD_IN
+ * width) falls back to the next.  The 32-channel forms give identical
+ * results; FWD_IN's forms sum the taps in other groupings (fp32).  Not
+ * thread-safe against concurrent launches. */
+enum { LPBF_SG_FORM_ROWS = 0, LPBF_SG_FORM_TILES = 1, LPBF_SG_FORM_PLAIN = 2 };
+int lpbf_b200_sg_set_form(int form);
+/* Form that ran the last FWD_IN or 32-channel launch of this process (-1:
+ * none yet). */
+int lpbf_b200_sg_form_used(void);
 /* ---- The network: parameters, training, features ----------------------------
  * 5 layers (4 -> 32 -> 32 -> 32 -> 32 -> 1 channels, GELU after the first
  * four).  Inputs per pixel, bf16 NHWC: (T - T_amb) / LPBF_SG_T_SCALE, the

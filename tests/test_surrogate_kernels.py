@@ -218,3 +218,54 @@ def test_features_and_apply(gpu):
     assert np.allclose(T1.cpu().numpy(), T + 100.0 * y.cpu().numpy().astype(np.float64))
     t = target(Td, T1).cpu().numpy()
     assert np.allclose(t, y.cpu().numpy(), rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("B,H,W", [(2, 70, 260), (1, 33, 128), (3, 1, 90), (1, 4, 131)])
+def test_conv_forms_agree(gpu, B, H, W):
+    """The row-streaming, tap-tile and plain forms against the FP64
+    restatement on images with ragged row runs (H not a multiple of 32),
+    ragged column tiles and an odd width (the input layer's row form needs
+    an even one and falls back); the 32-channel forms agree bit for bit."""
+    from hedgehog_lpbf_b200 import _lib
+    L = _lib.lib()
+    rng = np.random.default_rng(7)
+    ps = R.init_params(11)
+    x4 = _bf16(rng.normal(size=(B, H, W, 4)))
+    act = _bf16(rng.normal(size=(B, H, W, 32)))
+    pre_prev = _bf16(rng.normal(size=(B, H, W, 32)))
+    b = rng.normal(size=32) * 0.1
+    w0, w1, w4 = ps[0][0], ps[1][0], ps[4][0]
+    w0q = _np(_bf16(w0.reshape(32, -1))).reshape(w0.shape)
+    w1q = _np(_bf16(w1.reshape(32, -1))).reshape(w1.shape)
+    w4q = _np(_bf16(w4.reshape(1, -1))).reshape(w4.shape)
+    wt = R.flip_transpose(ps[2][0])
+    wtq = _np(_bf16(wt.reshape(32, -1))).reshape(wt.shape)
+    ref_in = R.conv3x3(_np(x4), w0q, b)
+    ref_pre = R.conv3x3(_np(act), w1q, b)
+    ref_y = R.conv3x3(_np(act), w4q, np.array([0.25]))[..., 0]
+    ref_dx = R.conv3x3(_np(act), wtq) * R.gelu_grad(_np(pre_prev))
+    got = {}
+    try:
+        for form in (0, 1, 2):
+            assert L.lpbf_b200_sg_set_form(form) == 0
+            act0, pre0 = _conv(0, x4, _bf16(R.pack(w0, k_pad=64)), bias=b, want_pre=True)
+            assert L.lpbf_b200_sg_form_used() == (2 if form or W % 2 else 0)
+            _close(_np(pre0), ref_in)
+            _close(_np(act0), R.gelu(_np(pre0)))
+            act2, pre2 = _conv(1, act, _bf16(R.pack(w1)), bias=b, want_pre=True)
+            y, _ = _conv(2, act, _bf16(R.pack(w4, n_pad=16)), bias=np.array([0.25]),
+                         out_fp32=True)
+            dx, _ = _conv(4, act, _bf16(R.pack(wt)), pre_in=pre_prev)
+            assert L.lpbf_b200_sg_form_used() == form
+            _close(_np(pre2), ref_pre)
+            _close(_np(act2), R.gelu(_np(pre2)))
+            _close(_np(y), ref_y, rtol=2e-3)
+            _close(_np(dx), ref_dx)
+            got[form] = [_np(t) for t in (pre2, act2, y, dx)]
+    finally:
+        L.lpbf_b200_sg_set_form(0)
+    # same operands, same tap order: the 32-channel forms agree bit for bit
+    for form in (1, 2):
+        for a, c in zip(got[0], got[form]):
+            assert np.array_equal(a, c)
+    assert L.lpbf_b200_sg_set_form(3) != 0
