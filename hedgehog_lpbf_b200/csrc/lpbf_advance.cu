@@ -192,11 +192,22 @@ cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const Laser
     int H = rows;
     if (H <= 0) {
         if (dynamic) {
-            // about three tasks per resident warp, 12..64 rows: tall tasks
-            // cost less halo, and the band split keeps the slow source-band
-            // tasks short whatever H is
-            const long long want = (long long)nrows * p.nstrips / (3ll * resident * ADV_WARPS);
-            H = (int)std::max(12ll, std::min(64ll, want));
+            // 12..64 rows.  The queue deals tasks to the resident warps in
+            // waves, so the launch lasts about (waves) x (rows a task
+            // computes, its own plus about 2K of halo): take the height with
+            // the least of that, the taller on a tie.  Tall tasks cost less
+            // halo; a last wave that is nearly empty costs a whole task (a
+            // 2048-row strip of an 8192-wide field: 41 rows, two waves,
+            // instead of 26 rows and a fourth wave of 7 % of the warps).
+            // The band split keeps the slow source-band tasks short
+            // whatever H is.
+            const long long warps = (long long)resident * ADV_WARPS;
+            long long best = -1;
+            for (int h = 12; h <= 64; ++h) {
+                const long long tasks = (long long)((nrows + h - 1) / h) * p.nstrips;
+                const long long cost = ((tasks + warps - 1) / warps) * (h + 2 * K);
+                if (best < 0 || cost <= best) { best = cost; H = h; }
+            }
         } else {
             const int want = std::max(1, (resident * ADV_WARPS) / p.nstrips);
             H = (nrows + want - 1) / want;

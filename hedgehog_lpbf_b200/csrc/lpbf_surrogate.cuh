@@ -141,15 +141,20 @@ __device__ __forceinline__ float tanh_approx(float x) {
 }
 constexpr float GELU_C = 0.7978845608028654f;      // sqrt(2 / pi)
 constexpr float GELU_A = 0.044715f;
+constexpr float GELU_CA = GELU_C * GELU_A;
+// u = x (C + C A x^2); gelu = x/2 + x/2 t (five FP32 operations and a tanh)
 __device__ __forceinline__ float gelu(float x) {
-    const float u = GELU_C * fmaf(GELU_A * x, x * x, x);
-    return 0.5f * x * (1.0f + tanh_approx(u));
+    const float u = x * fmaf(x * x, GELU_CA, GELU_C);
+    const float hx = 0.5f * x;
+    return fmaf(hx, tanh_approx(u), hx);
 }
+// gelu' = (1 + t)/2 + x/2 (1 - t^2) u', u' = C + 3 C A x^2
 __device__ __forceinline__ float gelu_grad(float x) {
     const float x2 = x * x;
-    const float t = tanh_approx(GELU_C * fmaf(GELU_A * x, x2, x));
-    const float du = GELU_C * fmaf(3.0f * GELU_A, x2, 1.0f);
-    return 0.5f * (1.0f + t) + 0.5f * x * fmaf(-t, t, 1.0f) * du;
+    const float t = tanh_approx(x * fmaf(x2, GELU_CA, GELU_C));
+    const float du = fmaf(x2, 3.0f * GELU_CA, GELU_C);
+    const float hx = 0.5f * x;
+    return fmaf(hx * fmaf(-t, t, 1.0f), du, fmaf(0.5f, t, 0.5f));
 }
 
 }  // namespace sg
