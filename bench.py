@@ -485,6 +485,17 @@ def superstep_leg(args, dev):
         out["forward_4096sq"]["frac_of_measured_bf16"] = out["forward_4096sq"]["tflops"] / peak
     else:   # earlier cuBLAS bf16 burst measurement on B200
         out["forward_4096sq"]["frac_of_fallback_bf16_1590"] = out["forward_4096sq"]["tflops"] / 1590.0
+    # 32-channel 3x3 layers do about 111 FLOP per byte they must move, below
+    # the B200's ridge (bf16 peak / HBM bandwidth, about 256): the forward is
+    # bound by HBM.  Bytes per pixel: features in (8), four 32-channel bf16
+    # activations written (4 x 64) and read by the next layer (4 x 64), y
+    # out (4).
+    fwd_bytes = px * (8 + 4 * 64 + 4 * 64 + 4)
+    hbm = measured_peaks()
+    gbs = fwd_bytes / (fwd_ms * 1e-3) / 1e9
+    out["forward_4096sq"]["roofline"] = {
+        "bound": "hbm", "algorithmic_bytes": fwd_bytes, "achieved": gbs, "unit": "GB/s",
+        "peak": hbm[0], "peak_source": hbm[1], "frac": gbs / hbm[0]}
     return out
 
 
