@@ -277,8 +277,12 @@ def _cli():
     f = sub.add_parser("forward", help="time the network's forward pass on a side x side field")
     f.add_argument("--side", type=int, default=4096)
     f.add_argument("--reps", type=int, default=5)
+    f.add_argument("--form", type=int, default=0,
+                   help="layer kernel form (lpbf_b200_sg_set_form: 0 rows, 1 tap tiles, 2 plain)")
     a = ap.parse_args()
     if a.cmd == "forward":
+        from . import _lib
+        _lib.check(_lib.lib().lpbf_b200_sg_set_form(a.form), "sg_set_form")
         net = load()[0] if os.path.exists(WEIGHTS) else Net(init_params(0))
         mat, pr = P.benchmark_material_process()
         dom = P.square_domain(a.side)
@@ -296,8 +300,8 @@ def _cli():
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / a.reps
         flop = 2 * 9 * (4 * 32 + 3 * 32 * 32 + 32) * a.side * a.side
-        print(json.dumps({"side": a.side, "ms": ms, "tflops": flop / (ms * 1e-3) / 1e12,
-                          "error_word": net.error_word()}))
+        print(json.dumps({"side": a.side, "form": a.form, "ms": ms,
+                          "tflops": flop / (ms * 1e-3) / 1e12, "error_word": net.error_word()}))
         return
     t0 = time.time()
     ds = make_dataset(a.trajectories, a.steps, side=a.side, first_index=0)
