@@ -749,6 +749,258 @@ conv_row_kernel(const __grid_constant__ CUtensorMap xmap, const ConvArgs a, int 
     if (warp == 1) tmem_free(tmem, CR_NACC * ACC_COLS);
 }
 
+// ---- weight gradient of the 32 -> 32 layers, row-streaming ---------------------
+//
+// dW[co][(dy, dx, ci)] = sum over pixels p of g[p][co] x[p + (dy - 1, dx - 1)][ci]
+// and db[co] = sum of g[p][co].  The same runs of output rows as the
+// forward form; warp 0 streams the run's input rows (130 pixels, 64-byte
+// swizzle) and its gradient rows (128 pixels) by TMA.  Both operands are
+// read MN-major straight from those slots: for input row dy the A operand
+// is M = 128 = four 32-channel blocks 64 bytes apart (block dx is the row
+// shifted by dx pixels; the fourth is computed and dropped), K = 16 pixels;
+// B is the gradient row, N = 32 channels, K = 16 pixels.  Eight MMAs per
+// output row and dy accumulate into one of three TMEM accumulators (one per
+// dy) for the CTA's whole share; the eight epilogue warps sum the bias
+// gradient from the gradient slots meanwhile, and at the end write the
+// CTA's partial record, which a second kernel sums over CTAs in a fixed
+// order (deterministic).
+constexpr int WR_XS = 4;                           // input-row slots
+constexpr int WR_GS = 3;                           // gradient-row slots
+constexpr int WR_GBYTES = 128 * 64;                // one gradient row
+constexpr int WR_REC = 3 * 96 * 32 + 32;           // floats per CTA record
+constexpr int WR_MAX_CTAS = 1024;
+static_assert(CR_PITCH32 >= 131 * 64, "the dropped fourth block reads pixel 130");
+
+size_t wgrad_rows_scratch(long long P) {
+    return size_t(std::min<long long>(P, WR_MAX_CTAS)) * WR_REC * sizeof(float);
+}
+
+__device__ __forceinline__ uint64_t sw64_desc(const void* p, uint32_t lbo, uint32_t sbo) {
+    cute::UMMA::SmemDescriptor d;
+    d.version_ = 1;
+    d.lbo_mode_ = 0;
+    d.layout_type_ = uint8_t(cute::UMMA::LayoutType::SWIZZLE_64B);
+    d.start_address_ = uint16_t(smem_u32(p) >> 4);
+    d.base_offset_ = 0;
+    d.leading_byte_offset_ = uint16_t(lbo >> 4);
+    d.stride_byte_offset_ = uint16_t(sbo >> 4);
+    return d;
+}
+
+__global__ void __launch_bounds__(CT_THREADS, CR_CTAS)
+wgrad_row_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap gmap,
+                 const ConvArgs a, float* partial, int nunits, int xtiles, int runs) {
+    using Mma = cute::SM100_MMA_F16BF16_SS<bf16, bf16, float, 128, 32, cute::UMMA::Major::MN,
+                                           cute::UMMA::Major::MN>;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ uint64_t xfull[WR_XS], xempty[WR_XS], gfull[WR_GS], gempty[WR_GS], done;
+    __shared__ uint32_t tslot;
+    __shared__ float sbias[CT_EPI_WARPS][32];
+    uint8_t* base = align1024(smem_raw);
+    uint8_t* sX = base;
+    uint8_t* sG = base + size_t(WR_XS) * CR_PITCH32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (warp == 1) tmem_alloc(&tslot, 128);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < WR_XS; ++i) { mbar_init(&xfull[i], 1); mbar_init(&xempty[i], 1); }
+        for (int i = 0; i < WR_GS; ++i) {
+            mbar_init(&gfull[i], 1);
+            mbar_init(&gempty[i], 1 + CT_EPI_WARPS);   // the MMAs' commit, the bias warps
+        }
+        mbar_init(&done, 1);
+        fence_mbar_init();
+    }
+    // the bytes past the loaded 130 pixels of each input slot (read by the
+    // dropped fourth block only) hold zeros, not stale values
+    for (int i = threadIdx.x; i < WR_XS * (CR_PITCH32 - CR_ROW_BYTES) / 16; i += blockDim.x) {
+        const int s = i / ((CR_PITCH32 - CR_ROW_BYTES) / 16), o = i % ((CR_PITCH32 - CR_ROW_BYTES) / 16);
+        *reinterpret_cast<uint4*>(sX + size_t(s) * CR_PITCH32 + CR_ROW_BYTES + o * 16) =
+            make_uint4(0u, 0u, 0u, 0u);
+    }
+    fence_smem_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tslot;
+    bool ok = true;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            uint32_t gx = 0, gg = 0;                 // rows issued into each ring
+            for (int u = blockIdx.x; ok && u < nunits; u += gridDim.x) {
+                const RowUnit r = row_unit(u, xtiles, runs, a.H);
+                for (int L = 0; L < r.n + 2 && ok; ++L) {
+                    uint32_t s = gx % WR_XS;
+                    if (!mbar_wait_bounded(&xempty[s], ((gx / WR_XS) & 1) ^ 1)) { ok = false; break; }
+                    mbar_expect_tx(&xfull[s], CR_ROW_BYTES);
+                    tma_load_4d(sX + size_t(s) * CR_PITCH32, &xmap, 0, r.xt * 128 - 1,
+                                r.y0 - 1 + L, r.b, &xfull[s]);
+                    ++gx;
+                    if (L < 2) continue;
+                    s = gg % WR_GS;
+                    if (!mbar_wait_bounded(&gempty[s], ((gg / WR_GS) & 1) ^ 1)) { ok = false; break; }
+                    mbar_expect_tx(&gfull[s], WR_GBYTES);
+                    tma_load_4d(sG + size_t(s) * WR_GBYTES, &gmap, 0, r.xt * 128, r.y0 + L - 2, r.b,
+                                &gfull[s]);
+                    ++gg;
+                }
+            }
+            // the last copy issued into each slot has landed
+            for (uint32_t i = 0; i < WR_XS && i < gx; ++i) {
+                const uint32_t gi = gx - 1 - i;
+                if (!mbar_wait_bounded(&xfull[gi % WR_XS], (gi / WR_XS) & 1)) ok = false;
+            }
+            for (uint32_t i = 0; i < WR_GS && i < gg; ++i) {
+                const uint32_t gi = gg - 1 - i;
+                if (!mbar_wait_bounded(&gfull[gi % WR_GS], (gi / WR_GS) & 1)) ok = false;
+            }
+        }
+    } else if (warp == 1) {
+        const uint64_t idesc =
+            cute::UMMA::make_runtime_instr_desc<bf16, bf16, float, 128, 32, cute::UMMA::Major::MN,
+                                                cute::UMMA::Major::MN>();
+        // MN-major, 64-byte swizzle: 32-channel blocks 64 bytes apart (LBO),
+        // 8-pixel groups 512 bytes apart (SBO); in 16-byte units below
+        const uint64_t dX0 = sw64_desc(sX, 64, 512), dG0 = sw64_desc(sG, 64, 512);
+        uint32_t gx = 0, gg = 0;
+        bool first = true;
+        for (int u = blockIdx.x; ok && u < nunits; u += gridDim.x) {
+            const RowUnit r = row_unit(u, xtiles, runs, a.H);
+            for (int j = 0; j < r.n; ++j, ++gg) {
+                bool w = mbar_wait_bounded(&gfull[gg % WR_GS], (gg / WR_GS) & 1);
+#pragma unroll
+                for (int dy = 0; dy < 3; ++dy) {
+                    const uint32_t gi = gx + j + dy;
+                    w = w && mbar_wait_bounded(&xfull[gi % WR_XS], (gi / WR_XS) & 1);
+                }
+                if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
+                tc_fence_after();
+                const uint64_t dg = dG0 + (gg % WR_GS) * (WR_GBYTES >> 4);
+#pragma unroll
+                for (int dy = 0; dy < 3; ++dy) {
+                    const uint64_t dx = dX0 + ((gx + j + dy) % WR_XS) * (CR_PITCH32 >> 4);
+#pragma unroll
+                    for (int kk = 0; kk < 8; ++kk)   // 16 pixels = 1024 bytes per step
+                        Mma::fma(dx + kk * 64, dg + kk * 64, tmem + dy * 32,
+                                 (first && kk == 0) ? 0u : 1u, idesc);
+                }
+                first = false;
+                cutlass::arch::umma_arrive(&gempty[gg % WR_GS]);
+                cutlass::arch::umma_arrive(&xempty[(gx + j) % WR_XS]);
+                if (j == r.n - 1) {
+                    cutlass::arch::umma_arrive(&xempty[(gx + j + 1) % WR_XS]);
+                    cutlass::arch::umma_arrive(&xempty[(gx + j + 2) % WR_XS]);
+                }
+            }
+            gx += r.n + 2;
+        }
+        // every MMA issued has completed before the accumulators are read or freed
+        cutlass::arch::umma_arrive(&done);
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&done, 0))) ok = false;
+    } else {
+        const int e = warp - 2;                      // epilogue warp 0..7
+        // bias gradient: warp e sums pixels 16e .. 16e + 15 of each gradient
+        // row, lane = channel (the 16-byte chunk of channels c / 8 of pixel
+        // px sits at chunk (c / 8) ^ ((px / 2) % 4) of its 64-byte row)
+        float bsum = 0.0f;
+        uint32_t gg = 0;
+        for (int u = blockIdx.x; ok && u < nunits; u += gridDim.x) {
+            const RowUnit r = row_unit(u, xtiles, runs, a.H);
+            for (int j = 0; j < r.n; ++j, ++gg) {
+                if (!__all_sync(0xffffffffu,
+                                mbar_wait_bounded(&gfull[gg % WR_GS], (gg / WR_GS) & 1))) {
+                    ok = false;
+                    break;
+                }
+                const uint8_t* gs = sG + size_t(gg % WR_GS) * WR_GBYTES;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int px = 16 * e + i;
+                    const uint16_t v = *reinterpret_cast<const uint16_t*>(
+                        gs + px * 64 + ((((lane >> 3) ^ (px >> 1)) & 3) << 4) + (lane & 7) * 2);
+                    bsum += __uint_as_float(uint32_t(v) << 16);
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&gempty[gg % WR_GS]);
+            }
+        }
+        sbias[e][lane] = bsum;
+        // the CTA's record: rows dx * 32 + ci of accumulator dy (TMEM lane
+        // quarter q = dx; the fourth quarter is the dropped block)
+        const int q = warp & 3, h = e >> 2;
+        const bool w = __all_sync(0xffffffffu, ok && mbar_wait_bounded(&done, 0));
+        tc_fence_after();
+        float* rec = partial + size_t(blockIdx.x) * WR_REC;
+        if (w && q < 3) {
+#pragma unroll
+            for (int dy = 0; dy < 3; ++dy) {
+                float v[16];
+                tmem_ld16(tmem + dy * 32 + 16 * h + (uint32_t(q * 32) << 16), v);
+                float4* dst = reinterpret_cast<float4*>(rec + (dy * 96 + q * 32 + lane) * 32 + 16 * h);
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    dst[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+            }
+        }
+        if (!w) ok = false;
+        asm volatile("bar.sync 1, %0;" :: "r"(32 * CT_EPI_WARPS) : "memory");
+        if (e == 0) {
+            float s = 0.0f;
+#pragma unroll
+            for (int i = 0; i < CT_EPI_WARPS; ++i) s += sbias[i][lane];
+            rec[9216 + lane] = s;
+        }
+    }
+    if (!ok && a.err) atomicOr(a.err, 1u);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) tmem_free(tmem, 128);
+}
+
+// dW[co][tap * 32 + ci] and db[co] from the CTA records, summed in CTA order.
+__global__ void wgrad_row_reduce(const float* partial, int nrec, float* dw, float* db) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= WR_REC) return;
+    float s = 0.0f;
+    for (int r = 0; r < nrec; ++r) s += partial[size_t(r) * WR_REC + e];
+    if (e < 9216) {
+        const int co = e & 31, row = e >> 5, dy = row / 96, m = row % 96;
+        dw[co * 288 + (dy * 3 + (m >> 5)) * 32 + (m & 31)] = s;
+    } else {
+        db[e - 9216] = s;
+    }
+}
+
+cudaError_t launch_wgrad_rows(const bf16* x, const bf16* g, int B, int H, int W, float* dw,
+                              float* db, float* partial, unsigned int* err, cudaStream_t s) {
+    CUtensorMap xm, gm;
+    if (reinterpret_cast<uintptr_t>(x) % 16 != 0 || reinterpret_cast<uintptr_t>(g) % 16 != 0 ||
+        !tensor_map_act_bf16(x, 32, W, H, B, CR_PX, &xm) ||
+        !tensor_map_act_bf16(g, 32, W, H, B, 128, &gm))
+        return cudaErrorNotSupported;
+    constexpr size_t smem = 1024 + size_t(WR_XS) * CR_PITCH32 + size_t(WR_GS) * WR_GBYTES;
+    static bool attr = false;
+    if (!attr) {
+        const cudaError_t e = cudaFuncSetAttribute(
+            wgrad_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const int xtiles = (W + 127) / 128;
+    const int runs = (H + CR_RUN - 1) / CR_RUN;
+    const long long nu = (long long)xtiles * runs * B;
+    const long long P = (long long)B * H * W;
+    if (nu >= (1ll << 31)) return cudaErrorInvalidValue;
+    const int grid = (int)std::min<long long>(
+        {nu, (long long)CR_CTAS * sm_count(), (long long)WR_MAX_CTAS, P});
+    ConvArgs a{};
+    a.B = B; a.H = H; a.W = W; a.err = err;
+    wgrad_row_kernel<<<grid, CT_THREADS, smem, s>>>(xm, gm, a, partial, (int)nu, xtiles, runs);
+    wgrad_row_reduce<<<(WR_REC + 255) / 256, 256, 0, s>>>(partial, grid, dw, db);
+    return cudaGetLastError();
+}
+
 template <int N, int EPI>
 cudaError_t launch_conv_tma(const ConvArgs& a, cudaStream_t s) {
     CUtensorMap map;

@@ -157,5 +157,17 @@ __device__ __forceinline__ float gelu_grad(float x) {
     return fmaf(hx * fmaf(-t, t, 1.0f), du, fmaf(0.5f, t, 0.5f));
 }
 
+// ---- entry points shared with the training code (lpbf_surrogate.cu) -----------
+
+// Layer kernel form (LPBF_SG_FORM_*), set by lpbf_b200_sg_set_form.
+extern int g_conv_form;
+// Weight and bias gradients of a 32 -> 32 layer in the row-streaming form
+// (x: layer input, g: pre-activation gradient, both NHWC bf16 with 32
+// channels; dw [32][288], db [32]); cudaErrorNotSupported when its tensor
+// maps cannot be made.  `partial` holds wgrad_rows_scratch(P) bytes.
+cudaError_t launch_wgrad_rows(const bf16* x, const bf16* g, int B, int H, int W, float* dw,
+                              float* db, float* partial, unsigned int* err, cudaStream_t s);
+size_t wgrad_rows_scratch(long long P);
+
 }  // namespace sg
 }  // namespace lpbf_b200

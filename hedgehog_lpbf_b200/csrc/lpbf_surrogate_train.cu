@@ -254,7 +254,17 @@ cudaError_t launch_wgrad(const bf16* x, const bf16* g, int B, int H, int W, floa
 
 size_t wgrad_scratch(long long P) {
     return std::max({wgrad_partial_bytes<4, 32>(P), wgrad_partial_bytes<32, 32>(P),
-                     wgrad_partial_bytes<32, 16>(P)});
+                     wgrad_partial_bytes<32, 16>(P), wgrad_rows_scratch(P)});
+}
+
+// 32 -> 32 layers: the row-streaming form unless another form is selected
+// or it cannot run.
+cudaError_t launch_wgrad32(const bf16* x, const bf16* g, int B, int H, int W, float* dw, float* db,
+                           float* partial, unsigned int* err, cudaStream_t s) {
+    cudaError_t e = g_conv_form == 0 ? launch_wgrad_rows(x, g, B, H, W, dw, db, partial, err, s)
+                                     : cudaErrorNotSupported;
+    if (e == cudaErrorNotSupported) e = launch_wgrad<32, 32>(x, g, B, H, W, dw, db, partial, err, s);
+    return e;
 }
 
 // ---- loss, AdamW, packing, features ---------------------------------------------
@@ -531,8 +541,8 @@ int lpbf_b200_sg_gradients(void* net, const void* x4, const float* target, int b
         const bf16* xin = l == 0 ? static_cast<const bf16*>(x4) : w.act[l - 1];
         e = (l == 0) ? launch_wgrad<4, 32>(xin, g, batch, height, width, G + L.w_off[0],
                                            G + L.b_off[0], w.partial, err, stream)
-                     : launch_wgrad<32, 32>(xin, g, batch, height, width, G + L.w_off[l],
-                                            G + L.b_off[l], w.partial, err, stream);
+                     : launch_wgrad32(xin, g, batch, height, width, G + L.w_off[l],
+                                      G + L.b_off[l], w.partial, err, stream);
         if (e != cudaSuccess) return LPBF_ERR_CUDA;
         if (l > 0) {
             st = conv(LPBF_SG_DX_HIDDEN, g, dxw(l), nullptr, w.pre[l - 1], nullptr, g2, batch,

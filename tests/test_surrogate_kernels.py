@@ -142,20 +142,28 @@ def _bf16_params(ps):
     return [(_np(_bf16(w.reshape(w.shape[0], -1))).reshape(w.shape), b) for w, b in ps]
 
 
-def test_weight_gradients_match_fp64_backward(gpu):
+@pytest.mark.parametrize("B,H,W,form", [(2, 6, 150, 0), (2, 6, 150, 1), (2, 70, 260, 0)])
+def test_weight_gradients_match_fp64_backward(gpu, B, H, W, form):
     """Gradient check: the GPU's loss and per-layer gradients (bf16 operands,
     fp32 accumulation) against the FP64 backward pass of oracle/surrogate_ref
-    on the same bf16-rounded inputs and weights."""
+    on the same bf16-rounded inputs and weights, with the row-streaming
+    layers and weight gradients (form 0; 70 rows: three runs of rows per
+    column tile) and the tap-tile ones (form 1)."""
     import torch
+    from hedgehog_lpbf_b200 import _lib
     from hedgehog_lpbf_b200.surrogate import Net, unflatten
+    L = _lib.lib()
     rng = np.random.default_rng(7)
-    B, H, W = 2, 6, 150
     ps = _rand_net(3)
     x4 = _bf16(rng.normal(size=(B, H, W, 4)))
     tgt = rng.normal(size=(B, H, W)).astype(np.float32)
     net = Net(ps, device="cuda:0")
-    loss = net.gradients(x4.cuda(), torch.tensor(tgt, device="cuda:0"))
-    torch.cuda.synchronize()
+    try:
+        assert L.lpbf_b200_sg_set_form(form) == 0
+        loss = net.gradients(x4.cuda(), torch.tensor(tgt, device="cuda:0"))
+        torch.cuda.synchronize()
+    finally:
+        L.lpbf_b200_sg_set_form(0)
     assert net.error_word() == 0
     g_gpu = unflatten(net.grads_vector())
     loss_ref, g_ref = R.loss_and_grads(_bf16_params(ps), _np(x4), tgt.astype(np.float64))
@@ -269,3 +277,36 @@ def test_conv_forms_agree(gpu, B, H, W):
         for a, c in zip(got[0], got[form]):
             assert np.array_equal(a, c)
     assert L.lpbf_b200_sg_set_form(3) != 0
+
+
+def test_weight_gradient_forms_agree_at_size(gpu):
+    """576 row runs (more than one per CTA of the row-streaming weight
+    gradient): its gradients against the tap-tile form's on 2.4 M pixels
+    (the same operands; fp32 sums in other orders)."""
+    import torch
+    from hedgehog_lpbf_b200 import _lib
+    from hedgehog_lpbf_b200.surrogate import Net, unflatten
+    L = _lib.lib()
+    rng = np.random.default_rng(9)
+    B, H, W = 24, 256, 384
+    ps = _rand_net(6)
+    x4 = _bf16(rng.normal(size=(B, H, W, 4))).cuda()
+    tgt = torch.tensor(rng.normal(size=(B, H, W)).astype(np.float32), device="cuda:0")
+    grads = {}
+    try:
+        for form in (0, 1):
+            assert L.lpbf_b200_sg_set_form(form) == 0
+            net = Net(ps, device="cuda:0")
+            net.gradients(x4, tgt)
+            torch.cuda.synchronize()
+            assert net.error_word() == 0
+            grads[form] = unflatten(net.grads_vector())
+            del net
+    finally:
+        L.lpbf_b200_sg_set_form(0)
+    for li in range(5):
+        for part in (0, 1):
+            a, b = grads[0][li][part].ravel(), grads[1][li][part].ravel()
+            rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+            cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
+            assert rel < 1e-2 and cos > 0.9999, (li, part, rel, cos)
