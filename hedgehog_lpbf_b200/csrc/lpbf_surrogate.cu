@@ -1001,6 +1001,179 @@ cudaError_t launch_wgrad_rows(const bf16* x, const bf16* g, int B, int H, int W,
     return cudaGetLastError();
 }
 
+// ---- weight gradients of the 4 -> 32 and 32 -> 1 layers, CUDA cores ---------
+//
+// Too narrow for 128-row tensor-core tiles (36 and 1 real rows): each thread
+// owns fixed sums over the pixels of its CTA's runs of rows, read from three
+// input rows and one gradient row staged in shared memory.
+//   32 -> 1 : 288 threads, one (tap, input channel) each; thread 0 also the
+//             bias.  Per pixel: one input value, one (broadcast) gradient.
+//   4 -> 32 : 148 of 160 threads, (tap, input channel) x 8 output channels,
+//             and 4 threads the bias of 8 channels each.
+// Each CTA writes its record in the gradient's own order (dW[co][tap][ci],
+// then db); a second kernel sums the records in CTA order.
+template <int CIN, int COUT>
+struct WgSmall {
+    static constexpr int NOUT = 9 * CIN * COUT + COUT;
+    static constexpr int THREADS = CIN == 32 ? 288 : 160;
+    static constexpr int RUN = 8;    // output rows per unit: enough CTAs to hide latency
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__((WgSmall<CIN, COUT>::THREADS))
+wgrad_small_kernel(const bf16* __restrict__ x, const bf16* __restrict__ g, int H, int W,
+                   int nunits, int xtiles, int runs, float* partial) {
+    static_assert((CIN == 32 && COUT == 1) || (CIN == 4 && COUT == 32), "narrow layers");
+    constexpr int NOUT = WgSmall<CIN, COUT>::NOUT;
+    // input rows as bf16 (pixel p of a slot is column xt * 128 - 1 + p), the
+    // gradient row as fp32
+    __shared__ __align__(16) uint16_t sx[3][CR_PX][CIN];
+    __shared__ __align__(16) float sg[128][COUT];
+    const int t = threadIdx.x;
+    // outputs of this thread
+    int tap = 0, ci = 0, cb = 0;
+    bool bias = false, active = true;
+    if constexpr (CIN == 32) {
+        tap = t >> 5;
+        ci = t & 31;
+        bias = t == 0;
+    } else {
+        const int tc = t >> 2;
+        cb = (t & 3) * 8;
+        active = tc <= 36;
+        bias = tc == 36;
+        tap = bias ? 0 : tc >> 2;
+        ci = tc & 3;
+    }
+    const int dy = tap / 3, dx = tap % 3;
+    float acc[COUT == 32 ? 8 : 1];
+    float bacc = 0.0f;
+#pragma unroll
+    for (int c = 0; c < (COUT == 32 ? 8 : 1); ++c) acc[c] = 0.0f;
+
+    auto stage_x = [&](int slot, int b, int y, int x0) {
+        // 16-byte units of CIN channels: CIN = 32: 4 per pixel; CIN = 4: half
+        // a unit per pixel, so 8-byte units
+        if constexpr (CIN == 32) {
+            for (int i = t; i < CR_PX * 4; i += blockDim.x) {
+                const int p = i >> 2, q = i & 3, xx = x0 - 1 + p;
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (y >= 0 && y < H && xx >= 0 && xx < W)
+                    v = __ldg(reinterpret_cast<const uint4*>(
+                        x + ((size_t(b) * H + y) * W + xx) * 32 + q * 8));
+                *reinterpret_cast<uint4*>(&sx[slot][p][q * 8]) = v;
+            }
+        } else {
+            for (int p = t; p < CR_PX; p += blockDim.x) {
+                const int xx = x0 - 1 + p;
+                uint2 v = make_uint2(0u, 0u);
+                if (y >= 0 && y < H && xx >= 0 && xx < W)
+                    v = __ldg(reinterpret_cast<const uint2*>(x + ((size_t(b) * H + y) * W + xx) * 4));
+                *reinterpret_cast<uint2*>(&sx[slot][p][0]) = v;
+            }
+        }
+    };
+    auto stage_g = [&](int b, int y, int x0) {
+        for (int i = t; i < 128 * COUT; i += blockDim.x) {
+            const int p = i / COUT, c = i % COUT, xx = x0 + p;
+            float v = 0.0f;
+            if (xx < W) {
+                const uint16_t u = reinterpret_cast<const uint16_t*>(g)[((size_t(b) * H + y) * W + xx) * COUT + c];
+                v = __uint_as_float(uint32_t(u) << 16);
+            }
+            sg[p][c] = v;
+        }
+    };
+
+    constexpr int RUN = WgSmall<CIN, COUT>::RUN;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        RowUnit r;
+        r.xt = u % xtiles;
+        r.b = (u / xtiles) / runs;
+        r.y0 = ((u / xtiles) % runs) * RUN;
+        r.n = min(RUN, H - r.y0);
+        const int x0 = r.xt * 128;
+        stage_x(0, r.b, r.y0 - 1, x0);
+        stage_x(1, r.b, r.y0, x0);
+        for (int j = 0; j < r.n; ++j) {
+            stage_x((j + 2) % 3, r.b, r.y0 + j + 1, x0);
+            stage_g(r.b, r.y0 + j, x0);
+            __syncthreads();
+            if (active) {
+                const uint16_t* xr = &sx[(j + dy) % 3][dx][ci];
+                if constexpr (COUT == 1) {
+#pragma unroll 8
+                    for (int p = 0; p < 128; ++p) {
+                        const float gv = sg[p][0];
+                        acc[0] = fmaf(__uint_as_float(uint32_t(xr[p * CIN]) << 16), gv, acc[0]);
+                        if (bias) bacc += gv;
+                    }
+                } else {
+#pragma unroll 4
+                    for (int p = 0; p < 128; ++p) {
+                        const float4 g0 = *reinterpret_cast<const float4*>(&sg[p][cb]);
+                        const float4 g1 = *reinterpret_cast<const float4*>(&sg[p][cb + 4]);
+                        const float xv = bias ? 1.0f : __uint_as_float(uint32_t(xr[p * CIN]) << 16);
+                        acc[0] = fmaf(xv, g0.x, acc[0]); acc[1] = fmaf(xv, g0.y, acc[1]);
+                        acc[2] = fmaf(xv, g0.z, acc[2]); acc[3] = fmaf(xv, g0.w, acc[3]);
+                        acc[4] = fmaf(xv, g1.x, acc[4]); acc[5] = fmaf(xv, g1.y, acc[5]);
+                        acc[6] = fmaf(xv, g1.z, acc[6]); acc[7] = fmaf(xv, g1.w, acc[7]);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    float* rec = partial + size_t(blockIdx.x) * NOUT;
+    if constexpr (COUT == 1) {
+        rec[tap * 32 + ci] = acc[0];
+        if (bias) rec[288] = bacc;
+    } else if (active) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            if (bias) rec[9 * 4 * 32 + cb + c] = acc[c];
+            else      rec[(cb + c) * 36 + tap * 4 + ci] = acc[c];
+        }
+    }
+}
+
+template <int NOUT, int NW>
+__global__ void wgrad_small_reduce(const float* partial, int nrec, float* dw, float* db) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= NOUT) return;
+    float s = 0.0f;
+    for (int r = 0; r < nrec; ++r) s += partial[size_t(r) * NOUT + e];
+    if (e < NW) dw[e] = s;
+    else        db[e - NW] = s;
+}
+
+template <int CIN, int COUT>
+cudaError_t launch_wgrad_small(const bf16* x, const bf16* g, int B, int H, int W, float* dw,
+                               float* db, float* partial, cudaStream_t s) {
+    constexpr int NOUT = WgSmall<CIN, COUT>::NOUT;
+    if (reinterpret_cast<uintptr_t>(x) % 16 != 0) return cudaErrorNotSupported;
+    constexpr int RUN = WgSmall<CIN, COUT>::RUN;
+    const int xtiles = (W + 127) / 128;
+    const int runs = (H + RUN - 1) / RUN;
+    const long long nu = (long long)xtiles * runs * B;
+    const long long P = (long long)B * H * W;
+    if (nu >= (1ll << 31)) return cudaErrorInvalidValue;
+    const int grid = (int)std::min<long long>({nu, 8ll * sm_count(), (long long)WR_MAX_CTAS, P});
+    wgrad_small_kernel<CIN, COUT><<<grid, WgSmall<CIN, COUT>::THREADS, 0, s>>>(
+        x, g, H, W, (int)nu, xtiles, runs, partial);
+    wgrad_small_reduce<NOUT, 9 * CIN * COUT><<<(NOUT + 255) / 256, 256, 0, s>>>(partial, grid, dw, db);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wgrad_in(const bf16* x, const bf16* g, int B, int H, int W, float* dw, float* db,
+                            float* partial, cudaStream_t s) {
+    return launch_wgrad_small<4, 32>(x, g, B, H, W, dw, db, partial, s);
+}
+cudaError_t launch_wgrad_out(const bf16* x, const bf16* g, int B, int H, int W, float* dw,
+                             float* db, float* partial, cudaStream_t s) {
+    return launch_wgrad_small<32, 1>(x, g, B, H, W, dw, db, partial, s);
+}
+
 template <int N, int EPI>
 cudaError_t launch_conv_tma(const ConvArgs& a, cudaStream_t s) {
     CUtensorMap map;

@@ -168,6 +168,13 @@ extern int g_conv_form;
 cudaError_t launch_wgrad_rows(const bf16* x, const bf16* g, int B, int H, int W, float* dw,
                               float* db, float* partial, unsigned int* err, cudaStream_t s);
 size_t wgrad_rows_scratch(long long P);
+// Weight and bias gradients of the input (4 -> 32) and output (32 -> 1)
+// layers on CUDA cores, the same runs of rows; partial: wgrad_rows_scratch
+// bytes suffice.
+cudaError_t launch_wgrad_in(const bf16* x, const bf16* g, int B, int H, int W, float* dw, float* db,
+                            float* partial, cudaStream_t s);
+cudaError_t launch_wgrad_out(const bf16* x, const bf16* g, int B, int H, int W, float* dw,
+                             float* db, float* partial, cudaStream_t s);
 
 }  // namespace sg
 }  // namespace lpbf_b200

@@ -530,8 +530,13 @@ int lpbf_b200_sg_gradients(void* net, const void* x4, const float* target, int b
     float* G = reinterpret_cast<float*>(n + L.grads);
     auto dxw = [&](int l) { return reinterpret_cast<const bf16*>(n + L.dx[l]); };
     // layer 5 (32 -> 1): weight gradient, then the gradient into layer 4
-    cudaError_t e = launch_wgrad<32, 16>(w.act[3], w.g5, batch, height, width, G + L.w_off[4],
-                                         G + L.b_off[4], w.partial, err, stream);
+    cudaError_t e = g_conv_form == 0
+        ? launch_wgrad_out(w.act[3], w.g5, batch, height, width, G + L.w_off[4], G + L.b_off[4],
+                           w.partial, stream)
+        : cudaErrorNotSupported;
+    if (e == cudaErrorNotSupported)
+        e = launch_wgrad<32, 16>(w.act[3], w.g5, batch, height, width, G + L.w_off[4],
+                                 G + L.b_off[4], w.partial, err, stream);
     if (e != cudaSuccess) return LPBF_ERR_CUDA;
     st = conv(LPBF_SG_DX_OUT, w.g5, dxw(4), nullptr, w.pre[3], nullptr, w.ga, batch, height,
               width, err, stream);
@@ -539,10 +544,17 @@ int lpbf_b200_sg_gradients(void* net, const void* x4, const float* target, int b
     bf16* g2 = w.gb;
     for (int l = 3; l >= 0 && st == LPBF_OK; --l) {
         const bf16* xin = l == 0 ? static_cast<const bf16*>(x4) : w.act[l - 1];
-        e = (l == 0) ? launch_wgrad<4, 32>(xin, g, batch, height, width, G + L.w_off[0],
-                                           G + L.b_off[0], w.partial, err, stream)
-                     : launch_wgrad32(xin, g, batch, height, width, G + L.w_off[l],
-                                      G + L.b_off[l], w.partial, err, stream);
+        if (l == 0) {
+            e = g_conv_form == 0 ? launch_wgrad_in(xin, g, batch, height, width, G + L.w_off[0],
+                                                   G + L.b_off[0], w.partial, stream)
+                                 : cudaErrorNotSupported;
+            if (e == cudaErrorNotSupported)
+                e = launch_wgrad<4, 32>(xin, g, batch, height, width, G + L.w_off[0],
+                                        G + L.b_off[0], w.partial, err, stream);
+        } else {
+            e = launch_wgrad32(xin, g, batch, height, width, G + L.w_off[l], G + L.b_off[l],
+                               w.partial, err, stream);
+        }
         if (e != cudaSuccess) return LPBF_ERR_CUDA;
         if (l > 0) {
             st = conv(LPBF_SG_DX_HIDDEN, g, dxw(l), nullptr, w.pre[l - 1], nullptr, g2, batch,
