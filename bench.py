@@ -350,6 +350,31 @@ def process_map_leg(args, dev, rank=0, world=1):
     return out
 
 
+def dropin_leg(args, dev):
+    """The reference's per-step call sequence (its GpuStepTask batch loop:
+    step, reduce, finalize, hot-column extract, one ring copy and one sync
+    per 64 steps) over this library's drop-in C-ABI, on the bench field and
+    raster: what a reference build gets by linking this library in place of
+    its kernels.  Unfused and fused forms, 64 warm-up steps, then the timed
+    ones."""
+    import torch
+    from hedgehog_lpbf_b200 import dropin
+    mat, pr, dom, k, plan = workload(0)
+    n = args.dropin_steps
+    out = {"unit": "GCell-updates/s",
+           "what": "reference GpuStepTask call sequence (mode 2, batch 64) over this "
+                   "library's lpbf_launch_* entry points, CUDA events"}
+    for name, fused in (("unfused", False), ("fused", True)):
+        dropin.run(k, dom, plan[:64], mat.Tm, fused=fused, device=dev)
+        r = dropin.run(k, dom, plan[64:64 + n], mat.Tm, fused=fused, device=dev)
+        out[name] = {"value": r["gcell_updates_per_s"], "ms_per_step": r["ms_per_step"],
+                     "steps": n, "extract_col": r["extract_col"]}
+        del r
+        torch.cuda.empty_cache()
+    out["value"] = max(out["unfused"]["value"], out["fused"]["value"])
+    return out
+
+
 def ext_leg(args, dev):
     """Extended physics (phys = 1: Mills k(T), cp(T) with latent heat, the
     reference's StepTileTask extended branch) on the 8192^2 field: the
@@ -694,6 +719,7 @@ def run_b200_arm(args, rank, world, local_rank):
     run_sh = args.sharded and (world == 1 or args.shard_ranks)
     sh = sharded_leg(args, dev, rank, world, value / world) if run_sh else None
     ext = ext_leg(args, dev) if args.ext else None
+    di = dropin_leg(args, dev) if args.dropin else None
     pm = None
     if args.process_map:
         pm = process_map_leg(args, dev, rank, world)
@@ -743,6 +769,7 @@ def run_b200_arm(args, rank, world, local_rank):
         "gpu_launches": launches * args.steps,
         "f32k": f32k,
         "ext_physics": ext,
+        "dropin_abi": di,
         "process_map": pm,
         "sharded": sh,
         "superstep": ss,
@@ -765,6 +792,10 @@ def run_b200_arm(args, rank, world, local_rank):
             if rg.get("value"):
                 line["speedup_vs_ref_gpu"] = value / rg["value"]
                 line["e2e_speedup_vs_ref_gpu"] = e2e_value / rg["value"]
+                if di:
+                    # the same host call sequence: this library's kernels
+                    # against the reference's
+                    di["vs_ref_gpu_same_calls"] = di["value"] / rg["value"]
     print(json.dumps(line), flush=True)
 
 
@@ -784,6 +815,9 @@ def main():
                     help="skip the reference GPU task graph baseline")
     ap.add_argument("--no-f32k", dest="f32k", action="store_false",
                     help="skip the FP32 compensated leg")
+    ap.add_argument("--no-dropin", dest="dropin", action="store_false",
+                    help="skip the reference call-sequence leg over the drop-in C-ABI")
+    ap.add_argument("--dropin-steps", type=int, default=448)
     ap.add_argument("--no-ext", dest="ext", action="store_false",
                     help="skip the extended-physics leg")
     ap.add_argument("--ext-steps", type=int, default=300)

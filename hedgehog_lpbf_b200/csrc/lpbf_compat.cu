@@ -457,32 +457,74 @@ cudaError_t launch_ext_step(const double* Tin, double* Tout, const StepConst& k,
 }
 
 // ---- standalone reduce --------------------------------------------------------
-// Block b takes rows b, b + nblocks, ...; threads stride over the columns, so
-// each thread meets its cells in increasing index order.
-__global__ void __launch_bounds__(256)
+// Block b takes rows b, b + nblocks, ... (the reference's API fixes the grid
+// at nblocks Partials, 256 for large fields: under two CTAs per SM), so each
+// CTA keeps many bytes in flight: 1024 threads, each loading RR_VEC
+// independent 16-byte pairs of a row before examining them.  A thread meets
+// its cells in increasing index order (pairs in order, then the next group
+// of pairs, then the next row), so a strict '>' keeps its first maximal
+// cell; the block's threads then combine by the same rule as every Partial.
+constexpr int RR_THREADS = 1024;
+constexpr int RR_VEC = 4;
+
+__device__ __forceinline__ void rr_take(double v, long long i, double& tm, long long& ag,
+                                        bool& molten, double Tm) {
+    if (v > tm) { tm = v; ag = i; }
+    molten |= (v > Tm);
+}
+
+__global__ void __launch_bounds__(RR_THREADS)
 reduce_rows_kernel(const double* __restrict__ T, int nx, int ny, double Tm,
                    Partial* __restrict__ out) {
     const long long N = (long long)nx * ny;
     double tm = -1.0; long long ag = N; int mn = ny, mx = -1;
+    // 16-byte pairs when every row starts on a 16-byte boundary
+    const bool pairs = (nx % 2 == 0) && (reinterpret_cast<uintptr_t>(T) % 16 == 0);
     for (int y = blockIdx.x; y < ny; y += gridDim.x) {
         const double* row = T + (size_t)y * nx;
+        const long long base = (long long)y * nx;
         bool molten = false;
-        for (int x = threadIdx.x; x < nx; x += blockDim.x) {
-            const double v = __ldg(row + x);
-            if (v > tm) { tm = v; ag = (long long)y * nx + x; }
-            molten |= (v > Tm);
+        if (pairs) {
+            const double2* r2 = reinterpret_cast<const double2*>(row);
+            const int np = nx / 2;
+            for (int p0 = threadIdx.x; p0 < np; p0 += RR_THREADS * RR_VEC) {
+                double2 v[RR_VEC];
+#pragma unroll
+                for (int u = 0; u < RR_VEC; ++u) {
+                    const int p = p0 + u * RR_THREADS;
+                    v[u] = p < np ? __ldg(r2 + p) : make_double2(-INFINITY, -INFINITY);
+                }
+#pragma unroll
+                for (int u = 0; u < RR_VEC; ++u) {
+                    const long long i = base + 2ll * (p0 + u * RR_THREADS);
+                    rr_take(v[u].x, i, tm, ag, molten, Tm);
+                    rr_take(v[u].y, i + 1, tm, ag, molten, Tm);
+                }
+            }
+        } else {
+            for (int x0 = threadIdx.x; x0 < nx; x0 += RR_THREADS * RR_VEC) {
+                double v[RR_VEC];
+#pragma unroll
+                for (int u = 0; u < RR_VEC; ++u) {
+                    const int x = x0 + u * RR_THREADS;
+                    v[u] = x < nx ? __ldg(row + x) : -INFINITY;
+                }
+#pragma unroll
+                for (int u = 0; u < RR_VEC; ++u)
+                    rr_take(v[u], base + x0 + u * RR_THREADS, tm, ag, molten, Tm);
+            }
         }
         if (molten) { mn = min(mn, y); mx = max(mx, y); }
     }
     partial_warp_reduce(tm, ag, mn, mx);
-    __shared__ Partial red[8];
+    __shared__ Partial red[RR_THREADS / 32];
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = Partial{tm, ag, mn, mx};
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = -1.0; long long b = N; int c = ny, d = -1;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
-            partial_take(a, b, c, d, red[w].tmax, red[w].arg, red[w].ymin, red[w].ymax);
-        out[blockIdx.x] = Partial{a, b, c, d};
+    if (threadIdx.x < 32) {
+        Partial q = red[threadIdx.x];
+        double a = q.tmax; long long b = q.arg; int c = q.ymin, d = q.ymax;
+        partial_warp_reduce(a, b, c, d);
+        if (threadIdx.x == 0) out[blockIdx.x] = Partial{a, b, c, d};
     }
 }
 
@@ -550,7 +592,7 @@ void lpbf_launch_step(const double* Tin, double* Tout, const StepConst* k, int p
 void lpbf_launch_reduce(const double* T, int nx, int ny, double Tm, Partial* out,
                         int nblocks, cudaStream_t stream) {
     if (nblocks <= 0) return;
-    reduce_rows_kernel<<<nblocks, 256, 0, stream>>>(T, nx, ny, Tm, out);
+    reduce_rows_kernel<<<nblocks, RR_THREADS, 0, stream>>>(T, nx, ny, Tm, out);
 }
 
 void lpbf_launch_step_reduce(const double* Tin, double* Tout, const StepConst* k, int phys,
