@@ -875,24 +875,52 @@ advance_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ 
     __threadfence();
     if constexpr (REDUCE) {
         if (p.ring) {
+            // The whole GPU waits on this CTA: every thread issues the loads
+            // of all its CTA records (FIN_U CTAs x K levels) before combining
+            // any, so the pass costs about one L2 round trip per FIN_U
+            // records, not one per record.  The combine is commutative (ties
+            // to the smaller index), so the order does not change the result.
+            constexpr int FIN_U = 4;
+            double tm[K]; long long ag[K]; int mn[K], mx[K];
+#pragma unroll
+            for (int t = 0; t < K; ++t) { tm[t] = -1.0; ag[t] = N; mn[t] = p.gny; mx[t] = -1; }
+            for (int i0 = threadIdx.x; i0 < (int)gridDim.x; i0 += blockDim.x * FIN_U) {
+                Partial q[FIN_U][K];
+#pragma unroll
+                for (int u = 0; u < FIN_U; ++u) {
+                    const int i = i0 + u * (int)blockDim.x;
+#pragma unroll
+                    for (int t = 0; t < K; ++t) {
+                        if (i < (int)gridDim.x) {
+                            const Partial* r = &p.scratch[(size_t)i * K + t];
+                            q[u][t] = Partial{__ldcg(&r->tmax), __ldcg(&r->arg),
+                                              __ldcg(&r->ymin), __ldcg(&r->ymax)};
+                        } else {
+                            q[u][t] = Partial{-1.0, N, p.gny, -1};
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < FIN_U; ++u)
+#pragma unroll
+                    for (int t = 0; t < K; ++t)
+                        partial_take(tm[t], ag[t], mn[t], mx[t], q[u][t].tmax, q[u][t].arg,
+                                     q[u][t].ymin, q[u][t].ymax);
+            }
+            __syncthreads();
+#pragma unroll
             for (int t = 0; t < K; ++t) {
-                double tm = -1.0; long long ag = N; int mn = p.gny, mx = -1;
-                for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
-                    const Partial* q = &p.scratch[(size_t)i * K + t];
-                    partial_take(tm, ag, mn, mx, __ldcg(&q->tmax), __ldcg(&q->arg),
-                                 __ldcg(&q->ymin), __ldcg(&q->ymax));
-                }
-                partial_warp_reduce(tm, ag, mn, mx);
-                __syncthreads();
-                if (lane == 0) red[wid][0] = Partial{tm, ag, mn, mx};
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    double a = -1.0; long long b = N; int c1 = p.gny, d1 = -1;
-                    for (int w = 0; w < ADV_WARPS; ++w)
-                        partial_take(a, b, c1, d1, red[w][0].tmax, red[w][0].arg,
-                                     red[w][0].ymin, red[w][0].ymax);
-                    p.ring[t] = Partial{a, b, c1, d1};
-                }
+                partial_warp_reduce(tm[t], ag[t], mn[t], mx[t]);
+                if (lane == 0) red[wid][t] = Partial{tm[t], ag[t], mn[t], mx[t]};
+            }
+            __syncthreads();
+            if (threadIdx.x < K) {
+                const int t = threadIdx.x;
+                double a = -1.0; long long b = N; int c1 = p.gny, d1 = -1;
+                for (int w = 0; w < ADV_WARPS; ++w)
+                    partial_take(a, b, c1, d1, red[w][t].tmax, red[w][t].arg,
+                                 red[w][t].ymin, red[w][t].ymax);
+                p.ring[t] = Partial{a, b, c1, d1};
             }
         }
     }

@@ -980,13 +980,7 @@ cudaError_t launch_wgrad_rows(const bf16* x, const bf16* g, int B, int H, int W,
         !tensor_map_act_bf16(g, 32, W, H, B, 128, &gm))
         return cudaErrorNotSupported;
     constexpr size_t smem = 1024 + size_t(WR_XS) * CR_PITCH32 + size_t(WR_GS) * WR_GBYTES;
-    static bool attr = false;
-    if (!attr) {
-        const cudaError_t e = cudaFuncSetAttribute(
-            wgrad_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    if (const cudaError_t e = smem_opt_in<wgrad_row_kernel>(smem); e != cudaSuccess) return e;
     const int xtiles = (W + 127) / 128;
     const int runs = (H + CR_RUN - 1) / CR_RUN;
     const long long nu = (long long)xtiles * runs * B;
@@ -1182,13 +1176,8 @@ cudaError_t launch_conv_tma(const ConvArgs& a, cudaStream_t s) {
         return cudaErrorNotSupported;
     constexpr size_t smem = ct_smem_bytes<N>();
     auto kern = conv_tma_kernel<N, EPI>;
-    static bool attr = false;
-    if (!attr) {
-        const cudaError_t e =
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    if (const cudaError_t e = smem_opt_in<conv_tma_kernel<N, EPI>>(smem); e != cudaSuccess)
+        return e;
     const int xtiles = (a.W + 127) / 128;
     const long long nt = (long long)xtiles * a.H * a.B;
     if (nt >= (1ll << 31)) return cudaErrorInvalidValue;
@@ -1207,13 +1196,8 @@ cudaError_t launch_conv_row(const ConvArgs& a, cudaStream_t s) {
         return cudaErrorNotSupported;
     constexpr size_t smem = cr_smem_bytes<CIN, N>();
     auto kern = conv_row_kernel<CIN, N, EPI>;
-    static bool attr = false;
-    if (!attr) {
-        const cudaError_t e =
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    if (const cudaError_t e = smem_opt_in<conv_row_kernel<CIN, N, EPI>>(smem); e != cudaSuccess)
+        return e;
     const int xtiles = (a.W + 127) / 128;
     const int runs = (a.H + CR_RUN - 1) / CR_RUN;
     const long long nu = (long long)xtiles * runs * a.B;
@@ -1227,13 +1211,8 @@ template <int CIN, int N, int EPI>
 cudaError_t launch_conv(const ConvArgs& a, cudaStream_t s) {
     constexpr size_t smem = conv_smem_bytes<CIN, N>();
     auto kern = conv_kernel<CIN, N, EPI>;
-    static bool attr = false;
-    if (!attr) {
-        const cudaError_t e =
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    if (const cudaError_t e = smem_opt_in<conv_kernel<CIN, N, EPI>>(smem); e != cudaSuccess)
+        return e;
     const dim3 grid((a.W + 127) / 128, a.H, a.B);
     kern<<<grid, 128, smem, s>>>(a);
     return cudaGetLastError();

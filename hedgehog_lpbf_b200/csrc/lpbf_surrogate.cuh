@@ -157,6 +157,20 @@ __device__ __forceinline__ float gelu_grad(float x) {
     return fmaf(hx * fmaf(-t, t, 1.0f), du, fmaf(0.5f, t, 0.5f));
 }
 
+// Opt kernel KERN in to `bytes` of dynamic shared memory on the current
+// device, once per device (the attribute belongs to each device's context).
+template <auto KERN>
+inline cudaError_t smem_opt_in(size_t bytes) {
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+    if (done[dev]) return cudaSuccess;
+    const cudaError_t e =
+        cudaFuncSetAttribute(KERN, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) done[dev] = true;
+    return e;
+}
+
 // ---- entry points shared with the training code (lpbf_surrogate.cu) -----------
 
 // Layer kernel form (LPBF_SG_FORM_*), set by lpbf_b200_sg_set_form.

@@ -232,13 +232,8 @@ cudaError_t launch_wgrad(const bf16* x, const bf16* g, int B, int H, int W, floa
                          float* partial, unsigned int* err, cudaStream_t s) {
     using T = TileMma<N, 64, 64>;
     constexpr size_t smem = 1024 + 2 * size_t(T::A_ELEMS + T::B_ELEMS) * 2;
-    static bool attr = false;
-    if (!attr) {
-        const cudaError_t e = cudaFuncSetAttribute(
-            wgrad_kernel<CIN, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    if (const cudaError_t e = smem_opt_in<wgrad_kernel<CIN, N>>(smem); e != cudaSuccess)
+        return e;
     WgArgs a;
     a.x = x; a.g = g; a.partial = partial; a.B = B; a.H = H; a.W = W;
     a.P = (long long)B * H * W;
