@@ -599,8 +599,9 @@ def sharded_leg(args, dev, rank=0, world=1, single_value=None):
     ms = max_over_ranks(e0.elapsed_time(e1), dev)
     out = {"value": dom.nx * dom.ny * n / (ms * 1e-3) / 1e9, "unit": "GCell-updates/s",
            "strips": parts, "halo_rows": depth, "exchange": kind, "time_steps": n, "ms": ms,
+           "launches": "one stream per strip" if world == 1 else "one strip per rank",
            "scaling": "strong (one field)" if world > 1 else "one GPU",
-           "error_word": f.stepper.read_error()}
+           "error_word": f.read_error()}
     parts_ring = f.partials(rings)
     if world == 1:
         s = Solver(k, device=dev, Tm=mat.Tm, depth=depth, T0=300.0)

@@ -180,7 +180,10 @@ class ShardedField:
     ``local(...)``: every strip in this process (strips exchange by copies);
     ``distributed(...)``: strip `rank` of `world`, one per rank.  `depth`
     steps per launch, and as many halo rows per side.  `stepper` advances
-    one strip by one launch (default: the CUDA kernel)."""
+    one strip by one launch (default: the CUDA kernel).  With the CUDA
+    kernel, the local form gives each strip its own stepper (workspace) and
+    stream, so the strips' launches overlap one another's start and tail;
+    the boundary rows are exchanged once all of a step's launches are done."""
 
     def __init__(self, k: StepConst, layout: list[Strip], mine: list[int], exchange,
                  stepper, *, depth: int, device: torch.device, T0=None, gather_fn=None):
@@ -191,6 +194,8 @@ class ShardedField:
         self.layout, self.mine = layout, mine
         self.strips = [layout[i] for i in mine]
         self.exchange, self.stepper = exchange, stepper
+        self.steppers = None               # per-strip steppers on their own streams
+        self._streams = None
         self.depth = self.halo = depth
         self.device = device
         self._gather_fn = gather_fn
@@ -206,9 +211,16 @@ class ShardedField:
               stepper=None, **opts) -> "ShardedField":
         dev = torch.device(device) if device is not None else torch.device("cuda")
         layout = strip_layout(k.ny, parts, depth)
-        step = stepper if stepper is not None else CudaStripStepper(dev, **opts)
-        return cls(k, layout, list(range(parts)), LocalExchange(), step, depth=depth,
-                   device=dev, T0=T0)
+        if stepper is not None:
+            return cls(k, layout, list(range(parts)), LocalExchange(), stepper, depth=depth,
+                       device=dev, T0=T0)
+        steps = [CudaStripStepper(dev, **opts) for _ in range(parts)]
+        f = cls(k, layout, list(range(parts)), LocalExchange(), steps[0], depth=depth,
+                device=dev, T0=T0)
+        if parts > 1:
+            f.steppers = steps
+            f._streams = [torch.cuda.Stream(device=dev) for _ in range(parts)]
+        return f
 
     @classmethod
     def distributed(cls, k: StepConst, rank: int, world: int, *, depth: int = 3, device=None,
@@ -252,13 +264,35 @@ class ShardedField:
                 for _ in self.strips] if rings else None)
         for s0 in range(0, n, self.depth):
             kk = min(self.depth, n - s0)
-            for i, s in enumerate(self.strips):
-                ring = out[i][24 * s0:24 * (s0 + kk)] if rings else None
-                self.stepper(self.bufs[i][self.cur], self.bufs[i][1 - self.cur], self.ks[i],
-                             self.ny, s, plan[s0:s0 + kk], ring)
+            if self._streams is not None:
+                main = torch.cuda.current_stream(self.device)
+                start = main.record_event()
+                done = []
+                for i, s in enumerate(self.strips):
+                    st = self._streams[i]
+                    st.wait_event(start)
+                    ring = out[i][24 * s0:24 * (s0 + kk)] if rings else None
+                    with torch.cuda.stream(st):
+                        self.steppers[i](self.bufs[i][self.cur], self.bufs[i][1 - self.cur],
+                                         self.ks[i], self.ny, s, plan[s0:s0 + kk], ring)
+                        done.append(st.record_event())
+                for e in done:
+                    main.wait_event(e)
+            else:
+                for i, s in enumerate(self.strips):
+                    ring = out[i][24 * s0:24 * (s0 + kk)] if rings else None
+                    self.stepper(self.bufs[i][self.cur], self.bufs[i][1 - self.cur], self.ks[i],
+                                 self.ny, s, plan[s0:s0 + kk], ring)
             self.cur = 1 - self.cur
             self.exchange(self.strips, [pair[self.cur] for pair in self.bufs], self.halo)
         return out
+
+    def read_error(self) -> int:
+        """The error words of this process's strip launches, or-ed."""
+        err = 0
+        for st in (self.steppers or [self.stepper]):
+            err |= st.read_error()
+        return err
 
     def partials(self, rings: list[torch.Tensor]) -> np.ndarray:
         """The field's per-step Partials from the strips' rings (collective

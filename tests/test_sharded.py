@@ -191,7 +191,7 @@ def test_gpu_strips_equal_the_single_field(gpu, nx, ny, parts, depth, bc):
     T = f.field().cpu().numpy()
     assert np.array_equal(T.view(np.uint64), T_ref.view(np.uint64))
     assert f.partials(rings).tobytes() == ring_to_numpy(ring_ref).tobytes()
-    assert f.stepper.read_error() == 0
+    assert f.read_error() == 0
     # and the oracle agrees with both
     from oracle import oracle as O
     T_o, _ = O.run(T0.ravel(), k, PL.laser_array(plan), bc=bc, T_D=300.0, Tm=mat.Tm)
