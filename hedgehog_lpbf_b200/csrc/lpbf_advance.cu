@@ -215,21 +215,9 @@ cudaError_t launch_t(const double* Tin, double* Tout, const Coef& c, const Laser
         H = std::max(H, std::max(8, 4 * K));
     }
     p.H = std::min(H, nrows);
-    p.Ya = p.Yb = p.row_lo;
-    p.Hb = p.H;
-    if (dynamic && p.band_lo <= p.band_hi) {
-        // rows whose tasks (owned rows +- K) reach the source band
-        const int b0 = std::max(p.row_lo, p.band_lo - K);
-        const int b1 = std::min(p.row_hi, p.band_hi + K + 1);
-        if (b0 < b1) {
-            p.Hb = std::min(p.H, ADV_BAND_ROWS);
-            p.nA = (b0 - p.row_lo) / p.H;
-            p.Ya = p.row_lo + p.nA * p.H;
-            p.Yb = b1;
-            p.nB = (p.Yb - p.Ya + p.Hb - 1) / p.Hb;
-        }
-    }
-    p.nchunks = p.nA + p.nB + (p.row_hi - p.Yb + p.H - 1) / p.H;
+    // the band split needs the dynamic queue (static scheduling: H-row chunks)
+    band_chunks(p.H, p.row_lo, p.row_hi, K, dynamic ? p.band_lo : 1, dynamic ? p.band_hi : 0,
+                &p.nA, &p.nB, &p.Hb, &p.Ya, &p.Yb, &p.nchunks);
     p.ntasks = p.nstrips * p.nchunks;
     int grid = std::min((p.ntasks + ADV_WARPS - 1) / ADV_WARPS, resident);
     if (REDUCE && !ref_out) grid = std::min(grid, std::min(MAX_CTAS, parts_cap / K));

@@ -94,6 +94,30 @@ struct AdvParams {
 
 __host__ __device__ constexpr int mod3(int a) { return ((a % 3) + 3) % 3; }
 
+// Chunk layout of rows [row_lo, row_hi) for tasks of H rows at depth K
+// (AdvParams's nA, nB, Hb, Ya, Yb, nchunks): the rows whose tasks (owned
+// rows +- K) reach the source band [band_lo, band_hi] go in chunks of at
+// most ADV_BAND_ROWS rows, so that none of these slow tasks is left long at
+// the end of a launch; H-row chunks before and after.  An empty band
+// (band_lo > band_hi) gives H-row chunks only.
+__host__ __device__ inline void band_chunks(int H, int row_lo, int row_hi, int K, int band_lo,
+                                            int band_hi, int* nA, int* nB, int* Hb, int* Ya,
+                                            int* Yb, int* nchunks) {
+    *nA = 0; *nB = 0; *Hb = H; *Ya = row_lo; *Yb = row_lo;
+    if (band_lo <= band_hi) {
+        const int b0 = band_lo - K > row_lo ? band_lo - K : row_lo;
+        const int b1 = band_hi + K + 1 < row_hi ? band_hi + K + 1 : row_hi;
+        if (b0 < b1) {
+            *Hb = H < ADV_BAND_ROWS ? H : ADV_BAND_ROWS;
+            *nA = (b0 - row_lo) / H;
+            *Ya = row_lo + *nA * H;
+            *Yb = b1;
+            *nB = (*Yb - *Ya + *Hb - 1) / *Hb;
+        }
+    }
+    *nchunks = *nA + *nB + (row_hi - *Yb + H - 1) / H;
+}
+
 // Hot coefficients, held in registers for the whole kernel (clsTa is
 // c_ls * Tamb, rounded once; sq: ax == ay, square cells).
 struct HotCoef {

@@ -188,6 +188,17 @@ batch_kernel(const __grid_constant__ BatchLaunch L) {
                     bxlo = min(bxlo, st.bandx_lo); bxhi = max(bxhi, st.bandx_hi);
                 }
                 par.band_lo = blo; par.band_hi = bhi; par.bandx_lo = bxlo; par.bandx_hi = bxhi;
+                // this launch's chunks: the band split of steps [step0, step0 +
+                // kfull), as the host's task tables count them
+                int ulo = 1 << 30, uhi = -(1 << 30);
+                const int tend = __ldg(&sc->split) ? min(L.step0 + L.kfull, L.nsteps) : 0;
+                for (int t = L.step0; t < tend; ++t) {
+                    const BatchStep& st = L.steps[(size_t)t * L.nscen + s];
+                    ulo = min(ulo, st.band_lo); uhi = max(uhi, st.band_hi);
+                }
+                band_chunks(par.H, 0, par.c.ny, L.kfull, ulo, uhi, &par.nA, &par.nB, &par.Hb,
+                            &par.Ya, &par.Yb, &par.nchunks);
+                par.ntasks = par.nstrips * par.nchunks;
                 par.Tin = sc->buf[L.parity];
                 par.Tout = sc->buf[L.parity ^ 1];
                 par.err = &L.hdr->err;
@@ -345,34 +356,85 @@ bool batch_layout(const lpbf_b200_scenario* sc, int n, int n_steps,
     std::stable_sort(Lo.order.begin(), Lo.order.end(), [&](int a, int b) {
         return (long long)sc[a].k->nx * sc[a].k->ny > (long long)sc[b].k->nx * sc[b].k->ny;
     });
-    Lo.task_base.assign(n + 1, 0);
-    Lo.group_base.assign(n + 1, 0);
     Lo.H.assign(n, 0);
-    long long tot = 0, gtot = 0;
+    Lo.split.assign(n, 0);
+    std::vector<int> nstrips(n), ny(n);
+    long long total = 0;
+    for (int i = 0; i < n; ++i) total += (long long)sc[i].k->nx * sc[i].k->ny;
+    bool plans = n_steps > 0;
     for (int i = 0; i < n; ++i) {
         const StepConst& k = *sc[Lo.order[i]].k;
-        const int H = resolve_rows(o, size_class(k.nx, k.ny), Lo.K, k.ny);
-        const long long nt = (long long)((k.nx + ADV_WOUT - 1) / ADV_WOUT) * ((k.ny + H - 1) / H);
-        Lo.H[i] = H;
-        Lo.task_base[i] = (int)tot;
-        Lo.group_base[i] = (int)gtot;
-        tot += nt;
-        gtot += (nt + BATCH_GROUP - 1) / BATCH_GROUP;
-        if (tot >= (1ll << 30)) return false;
+        Lo.H[i] = resolve_rows(o, size_class(k.nx, k.ny), Lo.K, k.ny);
+        nstrips[i] = (k.nx + ADV_WOUT - 1) / ADV_WOUT;
+        ny[i] = k.ny;
+        Lo.split[i] = batch_split_field((long long)k.nx * k.ny, total) ? 1 : 0;
+        plans = plans && sc[Lo.order[i]].plan != nullptr;
     }
-    Lo.task_base[n] = (int)tot;
-    Lo.group_base[n] = (int)gtot;
-    Lo.ntasks = (int)tot;
-    Lo.ngroups = (int)gtot;
+    // per-step laser data and source bands, by stored position
+    if (plans) {
+        Lo.steps.resize((size_t)n * n_steps);
+        for (int i = 0; i < n; ++i) {
+            const lpbf_b200_scenario& s = sc[Lo.order[i]];
+            const StepConst& k = *s.k;
+            const Coef c = make_coef(k, s.bc, s.T_edge, s.Tm);
+            for (int t = 0; t < n_steps; ++t) {
+                BatchStep& st = Lo.steps[(size_t)t * n + i];
+                st.las = make_laser(k, s.plan[t].x_l, s.plan[t].y_l, s.plan[t].q_scale);
+                laser_band(c, &st.las, 1, &st.band_lo, &st.band_hi, &st.bandx_lo, &st.bandx_hi);
+            }
+        }
+    }
+    // task and group offsets of every scenario for a launch starting at each
+    // plan step: the band split of the band over [r, r + K)
+    Lo.rows_t = std::max(n_steps, 1);
+    Lo.task_base.assign((size_t)Lo.rows_t * (n + 1), 0);
+    Lo.group_base.assign((size_t)Lo.rows_t * (n + 1), 0);
+    long long tmax = 0, gmax = 0;
+    for (int r = 0; r < Lo.rows_t; ++r) {
+        long long tot = 0, gtot = 0;
+        int* tb = &Lo.task_base[(size_t)r * (n + 1)];
+        int* gb = &Lo.group_base[(size_t)r * (n + 1)];
+        for (int i = 0; i < n; ++i) {
+            int lo = 1 << 30, hi = -(1 << 30);
+            if (plans && Lo.split[i]) {
+                for (int t = r; t < std::min(r + Lo.K, n_steps); ++t) {
+                    const BatchStep& st = Lo.steps[(size_t)t * n + i];
+                    lo = std::min(lo, st.band_lo);
+                    hi = std::max(hi, st.band_hi);
+                }
+            }
+            int nA, nB, Hb, Ya, Yb, nch;
+            band_chunks(Lo.H[i], 0, ny[i], Lo.K, lo, hi, &nA, &nB, &Hb, &Ya, &Yb, &nch);
+            long long nt = (long long)nstrips[i] * nch;
+            if (!plans) {
+                // sizing without the plans: every chunk of at most
+                // min(H, ADV_BAND_ROWS) rows bounds any launch's count
+                const int hb = std::min(Lo.H[i], ADV_BAND_ROWS);
+                nt = std::max(nt, (long long)nstrips[i] * ((ny[i] + hb - 1) / hb + 2));
+            }
+            tb[i] = (int)tot;
+            gb[i] = (int)gtot;
+            tot += nt;
+            gtot += (nt + BATCH_GROUP - 1) / BATCH_GROUP;
+            if (tot >= (1ll << 30)) return false;
+        }
+        tb[n] = (int)tot;
+        gb[n] = (int)gtot;
+        tmax = std::max(tmax, tot);
+        gmax = std::max(gmax, gtot);
+    }
+    Lo.ntasks = (int)tmax;
+    Lo.ngroups = (int)gmax;
+    const size_t tables = sizeof(int) * (size_t)Lo.rows_t * (n + 1);
     size_t off = sizeof(BatchHeader);
     Lo.off_done = off;   off = align_up(off + sizeof(unsigned int) * n, 256);
     Lo.off_scen = off;   off = align_up(off + sizeof(BatchScen) * n, 256);
-    Lo.off_base = off;   off = align_up(off + sizeof(int) * (n + 1), 256);
-    Lo.off_gbase = off;  off = align_up(off + sizeof(int) * (n + 1), 256);
-    Lo.off_gdone = off;  off = align_up(off + sizeof(unsigned int) * gtot, 256);
+    Lo.off_base = off;   off = align_up(off + tables, 256);
+    Lo.off_gbase = off;  off = align_up(off + tables, 256);
+    Lo.off_gdone = off;  off = align_up(off + sizeof(unsigned int) * gmax, 256);
     Lo.off_steps = off;  off = align_up(off + sizeof(BatchStep) * (size_t)n * n_steps, 256);
-    Lo.off_parts = off;  off = align_up(off + sizeof(Partial) * (size_t)tot * Lo.K, 256);
-    Lo.off_gparts = off; off = align_up(off + sizeof(Partial) * (size_t)gtot * Lo.K, 256);
+    Lo.off_parts = off;  off = align_up(off + sizeof(Partial) * (size_t)tmax * Lo.K, 256);
+    Lo.off_gparts = off; off = align_up(off + sizeof(Partial) * (size_t)gmax * Lo.K, 256);
     Lo.bytes = off;
     *out = std::move(Lo);
     return true;
@@ -455,20 +517,24 @@ struct lpbf_b200_batch {
 
     BatchLaunch launch_params(int step0, int parity) const {
         BatchLaunch L;
+        // the task tables of a launch starting at step0
+        const size_t row = (size_t)std::min(std::max(step0, 0), lay.rows_t - 1) * (nscen + 1);
         L.scen = reinterpret_cast<const BatchScen*>(work + lay.off_scen);
-        L.task_base = reinterpret_cast<const int*>(work + lay.off_base);
+        L.task_base = reinterpret_cast<const int*>(work + lay.off_base) + row;
         L.steps = reinterpret_cast<const BatchStep*>(work + lay.off_steps);
         L.hdr = reinterpret_cast<BatchHeader*>(work);
         L.scen_done = reinterpret_cast<unsigned int*>(work + lay.off_done);
-        L.group_base = reinterpret_cast<const int*>(work + lay.off_gbase);
+        L.group_base = reinterpret_cast<const int*>(work + lay.off_gbase) + row;
         L.group_done = reinterpret_cast<unsigned int*>(work + lay.off_gdone);
         L.parts = reinterpret_cast<Partial*>(work + lay.off_parts);
         L.gparts = reinterpret_cast<Partial*>(work + lay.off_gparts);
         L.nscen = nscen;
-        L.ntasks = lay.ntasks;
+        L.ntasks = lay.task_base[row + nscen];
         L.parity = parity;
         L.step0 = step0;
         L.sq_all = sq_all ? 1 : 0;
+        L.kfull = K;
+        L.nsteps = n_steps;
         return L;
     }
 
@@ -570,7 +636,7 @@ int lpbf_b200_batch_create(const lpbf_b200_scenario* sc, int n_scen, int n_steps
     std::vector<BatchHeader> img_store(img_bytes / sizeof(BatchHeader));
     unsigned char* img = reinterpret_cast<unsigned char*>(img_store.data());
     std::memset(img, 0, img_bytes);
-    std::vector<BatchStep> steps((size_t)n_scen * n_steps);
+    const std::vector<BatchStep>& steps = lay.steps;
     std::vector<BatchScen> scen(n_scen);
     bool sq_all = true;
     for (int i = 0; i < n_scen; ++i) {
@@ -595,19 +661,15 @@ int lpbf_b200_batch_create(const lpbf_b200_scenario* sc, int n_scen, int n_steps
         b.buf[1] = s.T_b;
         b.ring = s.ring;
         b.user = lay.order[i];
+        b.split = lay.split[i];
         if (stage == BATCH_STAGE_TMAP &&
             (!tensor_map_f64(s.T_a, k.nx, k.ny, ADV_COLS, ADV_R, &b.map[0]) ||
              !tensor_map_f64(s.T_b, k.nx, k.ny, ADV_COLS, ADV_R, &b.map[1])))
             return LPBF_ERR_TMA;
-        for (int t = 0; t < n_steps; ++t) {
-            BatchStep& st = steps[(size_t)t * n_scen + i];
-            st.las = make_laser(k, s.plan[t].x_l, s.plan[t].y_l, s.plan[t].q_scale);
-            laser_band(p.c, &st.las, 1, &st.band_lo, &st.band_hi, &st.bandx_lo, &st.bandx_hi);
-        }
     }
     std::memcpy(img + lay.off_scen, scen.data(), sizeof(BatchScen) * n_scen);
-    std::memcpy(img + lay.off_base, lay.task_base.data(), sizeof(int) * (n_scen + 1));
-    std::memcpy(img + lay.off_gbase, lay.group_base.data(), sizeof(int) * (n_scen + 1));
+    std::memcpy(img + lay.off_base, lay.task_base.data(), sizeof(int) * lay.task_base.size());
+    std::memcpy(img + lay.off_gbase, lay.group_base.data(), sizeof(int) * lay.group_base.size());
 
     int dev = 0;
     cudaGetDevice(&dev);

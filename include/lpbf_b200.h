@@ -212,7 +212,9 @@ typedef struct lpbf_b200_batch lpbf_b200_batch;   /* opaque host object */
 /* Size class of a grid for the per-class tile shape: 0 for max(nx, ny) < 512,
  * 1 for < 1024, 2 for < 2048, 3 above. */
 int lpbf_b200_batch_size_class(int nx, int ny);
-/* Device workspace bytes of a batch (0 for invalid arguments). */
+/* Device workspace bytes of a batch (0 for invalid arguments).  With every
+ * scenario's plan set this is exact; without plans it is an upper bound
+ * that holds whatever plans lpbf_b200_batch_create is later given. */
 size_t lpbf_b200_batch_workspace_bytes(const lpbf_b200_scenario* sc, int n_scen, int n_steps,
                                        const lpbf_b200_batch_opts* opts);
 /* Build a batch of n_scen scenarios sharing a step count.  work: 256-byte
@@ -243,8 +245,9 @@ int lpbf_b200_batch_run_wsub(lpbf_b200_batch* b, int first_step, int n_steps,
                              const unsigned char* cruise, double* w_sub, cudaStream_t stream);
 /* 1 when the current fields are in the T_b buffers, 0 for T_a. */
 int lpbf_b200_batch_result_in_b(const lpbf_b200_batch* b);
-/* Launches that a run of n_steps issues; queue items per launch; rows per
- * task chosen for a scenario (caller's index). */
+/* Launches that a run of n_steps issues; queue items of the largest launch
+ * (a scenario's rows near its laser go in shorter tasks, so the count
+ * follows the laser); rows per task chosen for a scenario (caller's index). */
 int lpbf_b200_batch_launches(const lpbf_b200_batch* b, int n_steps);
 int lpbf_b200_batch_tasks(const lpbf_b200_batch* b);
 int lpbf_b200_batch_scenario_rows(const lpbf_b200_batch* b, int scenario);

@@ -182,7 +182,7 @@ def test_autotune_trials_cache_and_tuned_batch(gpu, tmp_path):
     o1 = autotune(scs, n, cache=cache, trial_steps=6)
     d1 = opts_dict(o1)
     assert d1["depth"] in (2, 3, 4) and d1["staging"] in (1, 2)
-    assert all(r in (12, 24, 48, 96, 192) for r in d1["rows"])
+    assert all(r in (12, 24, 48, 96, 192, 384) for r in d1["rows"])
     doc = json.load(open(cache))
     assert tune_key(scs) in doc["entries"] and doc["entries"][tune_key(scs)]["gcells"] > 0
     t0 = time.time()

@@ -67,10 +67,12 @@ def test_batch_size_classes_and_workspace_bytes():
     assert [L.lpbf_b200_batch_size_class(s, s) for s in (256, 511, 512, 1024, 2047, 2048, 8192)] \
         == [0, 0, 1, 2, 2, 3, 3]
     assert L.lpbf_b200_batch_size_class(100, 3000) == 3
-    scs = PM.process_map(6, 10)
+    scs = PM.process_map(6, 20)
     arr = (_lib.Scenario * len(scs))()
+    plans = [np.ascontiguousarray(s.plan) for s in scs]
     for i, s in enumerate(scs):
         arr[i].k = ctypes.pointer(s.k)
+        arr[i].plan = plans[i].ctypes.data
     b1 = L.lpbf_b200_batch_workspace_bytes(arr, len(scs), 10, ctypes.byref(batch_opts(depth=3)))
     b2 = L.lpbf_b200_batch_workspace_bytes(arr, len(scs), 20, ctypes.byref(batch_opts(depth=3)))
     assert b1 > 0 and b1 % 256 == 0
@@ -78,6 +80,11 @@ def test_batch_size_classes_and_workspace_bytes():
     small = L.lpbf_b200_batch_workspace_bytes(arr, len(scs), 10,
                                               ctypes.byref(batch_opts(rows=(96, 96, 96, 96))))
     assert small < b1                             # fewer tasks, fewer partials
+    # without the plans the size is a bound that holds for any plan
+    for i in range(len(scs)):
+        arr[i].plan = None
+    assert L.lpbf_b200_batch_workspace_bytes(arr, len(scs), 10,
+                                             ctypes.byref(batch_opts(depth=3))) >= b1
     assert L.lpbf_b200_batch_workspace_bytes(arr, len(scs), 10,
                                              ctypes.byref(batch_opts(depth=9))) == 0
 
