@@ -25,6 +25,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import sys
@@ -491,10 +492,11 @@ def superstep_leg(args, dev):
                                 "tflops": 3 * FLOP_PER_PIXEL * 32 * 256 * 256 / (tr_ms * 1e-3) / 1e12},
         "hybrid_4096sq": {"steps": hyb["steps"], "hybrid_ms": hyb["gpu_ms"], "plain_fp64_ms": plain_ms,
                           "speedup_vs_plain": plain_ms / hyb["gpu_ms"],
-                          "max_abs_err_vs_fp64_K": float((Th - Tp).abs().max().item()),
+                          "max_abs_err_vs_fp64_K": _finite((Th - Tp).abs().max().item()),
                           "melt_area_err": abs(melt_h - melt_p) / max(melt_p, 1),
                           "judged": hyb["judged"], "rolled_back": hyb["rolled_back"],
-                          "worst_window_K": hyb["worst_K"]},
+                          "worst_window_K": _finite(hyb["worst_K"]),
+                          "full_fp64_blocks": hyb.get("full_fp64_blocks", 0)},
         "heldout": rec.get("heldout_trained") if rec else None,
     }
     del s, Tp, Th
@@ -524,6 +526,13 @@ def superstep_leg(args, dev):
     return out
 
 
+def _finite(v):
+    """A float for the JSON line, or None when it is not finite (strict JSON
+    has no NaN)."""
+    v = float(v)
+    return v if math.isfinite(v) else None
+
+
 def hybrid_scenarios(net, n_scen: int, n_steps: int, dev):
     """The batched part of the surrogate-in-the-loop workload: n_scen seeded
     process-map scenarios (grid side 256..2048, power, speed, spot, raster
@@ -546,23 +555,25 @@ def hybrid_scenarios(net, n_scen: int, n_steps: int, dev):
     e1.record()
     torch.cuda.synchronize()
     plain_ms = e0.elapsed_time(e1)
-    hyb_ms, worst, area_worst, judged, rolled = 0.0, 0.0, 0.0, 0, 0
+    hyb_ms, worst, area_worst, judged, rolled, full = 0.0, 0.0, 0.0, 0, 0, 0
     for i, sc in enumerate(scs):
         Th, r = run_hybrid(net, sc.k, sc.plan, np.full(sc.k.nx * sc.k.ny, sc.k.Tamb), n_steps,
                            judge_every=8, tol_K=5.0, area_tol=0.02, Tm=sc.Tm, device=dev)
         hyb_ms += r["gpu_ms"]
         judged += r["judged"]
         rolled += r["rolled_back"]
+        full += r["full_fp64_blocks"]
         Tp = b.field(i)
-        worst = max(worst, float((Th - Tp).abs().max().item()))
+        d = float((Th - Tp).abs().max().item())
+        worst = d if not math.isfinite(d) else max(worst, d)
         mp, mh = int((Tp > sc.Tm).sum().item()), int((Th > sc.Tm).sum().item())
         area_worst = max(area_worst, abs(mh - mp) / max(mp, 1) if (mp or mh) else 0.0)
         del Th
     b.close()
     return {"scenarios": n_scen, "steps_each": n_steps, "hybrid_ms": hyb_ms,
             "plain_fp64_batched_ms": plain_ms, "speedup_vs_plain": plain_ms / hyb_ms,
-            "max_abs_err_vs_fp64_K": worst, "worst_melt_area_err": area_worst,
-            "judged": judged, "rolled_back": rolled,
+            "max_abs_err_vs_fp64_K": _finite(worst), "worst_melt_area_err": area_worst,
+            "judged": judged, "rolled_back": rolled, "full_fp64_blocks": full,
             "note": "hybrid scenarios run one after another; the FP64 reference is the "
                     "batched kernel over all scenarios"}
 

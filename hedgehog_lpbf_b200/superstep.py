@@ -200,7 +200,7 @@ def _windows(plan, blocks: int, per_block: int, k, margin: int, halo: int):
 
 def run_hybrid(net: Net, k, plan, T0, n_steps: int, judge_every: int = 8, tol_K: float = 5.0,
                area_tol: float = 0.02, Tm: float = 1700.0, margin: int | None = None,
-               halo: int = 32, device="cuda:0"):
+               halo: int = 32, device="cuda:0", guard: bool = True):
     """Super-steps of the network with the FP64 judge and rollback.  Returns
     (field, record).
 
@@ -209,7 +209,21 @@ def run_hybrid(net: Net, k, plan, T0, n_steps: int, judge_every: int = 8, tol_K:
     solver for the whole run, so no buffers, workspace or tensor map are
     made per window); the verdict and the rollback (torch.where over the
     window) stay on the device, and the per-window records are read once at
-    the end."""
+    the end.
+
+    Outside the windows the network's errors accumulate unjudged, so every
+    block is also held to the discrete maximum principle: the laser heats
+    only inside the judged box, and the explicit step with its losses towards
+    Tamb/Tsub moves no cell above the largest or below the smallest of its
+    neighbourhood and those temperatures.  So after a block every cell lies
+    within [min(block-start field, Tamb, Tsub) - tol_K, max(block-start
+    field, FP64 box field, Tamb, Tsub) + tol_K].  A block whose field leaves
+    that range or is not finite is redone from its start with the FP64
+    solver over the whole field (counted in "full_fp64_blocks"); this keeps
+    the field inside the range in which the explicit step (whose radiation
+    term is unstable for very large T) stays finite.  The check reads one
+    flag per block on the host; ``guard=False`` leaves it out (the network's
+    own error outside the windows then shows in the field)."""
     dev = torch.device(device)
     if isinstance(T0, torch.Tensor):
         T = T0.to(dev, torch.float64).reshape(k.ny, k.nx).clone()
@@ -230,8 +244,14 @@ def run_hybrid(net: Net, k, plan, T0, n_steps: int, judge_every: int = 8, tol_K:
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     x4 = torch.empty((k.ny, k.nx, 4), dtype=torch.bfloat16, device=dev)
+    T_start = torch.empty_like(T)
+    full = None                  # FP64 solver over the whole field, made on first need
+    n_full = 0
+    t_lo, t_hi = min(k.Tamb, k.Tsub), max(k.Tamb, k.Tsub)
     for blk, (wy0, wy1, wx0, wx1, oy, ox) in enumerate(wins):
         s_blk = blk * per_block
+        T_start.copy_(T)
+        mn0, mx0 = torch.aminmax(T_start)
         fp64.set_field(T[oy:oy + bh, ox:ox + bw])
         for j in range(judge_every):
             s = s_blk + j * STEPS
@@ -243,6 +263,17 @@ def run_hybrid(net: Net, k, plan, T0, n_steps: int, judge_every: int = 8, tol_K:
         sub_plan["x_l"] -= ox * k.dx
         sub_plan["y_l"] -= oy * k.dy
         fp64.advance(sub_plan)
+        mn1, mx1 = torch.aminmax(T)
+        lo = torch.clamp(mn0, max=t_lo) - tol_K
+        hi = torch.maximum(mx0, fp64.field.max()).clamp(min=t_hi) + tol_K
+        ok = torch.isfinite(mn1) & torch.isfinite(mx1) & (mn1 >= lo) & (mx1 <= hi)
+        if guard and not bool(ok):
+            if full is None:
+                full = Solver(k, Tm=Tm, device=dev, T0=k.Tamb)
+            full.set_field(T_start)
+            full.advance(plan[s_blk:s_blk + per_block])
+            T.copy_(full.field)
+            n_full += 1
         ref = fp64.field[wy0 - oy:wy1 - oy, wx0 - ox:wx1 - ox]
         got = T[wy0:wy1, wx0:wx1]
         d, a, back = judge_device(got, ref, tol_K, area_tol, Tm)
@@ -256,6 +287,7 @@ def run_hybrid(net: Net, k, plan, T0, n_steps: int, judge_every: int = 8, tol_K:
            "worst_K": float(diffs[:blocks].max().item()) if blocks else 0.0,
            "worst_area": float(areas[:blocks].max().item()) if blocks else 0.0,
            "fp64_window_cells": blocks * bh * bw, "judge_box": [bh, bw],
+           "full_fp64_blocks": n_full,
            "gpu_ms": e0.elapsed_time(e1), "steps": blocks * per_block}
     return T, rec
 

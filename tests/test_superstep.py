@@ -58,9 +58,11 @@ def test_judge_rolls_back_to_fp64_in_the_window(small_training):
     T_ref = s.field.cpu().numpy()
     # a tolerance of 0 K rolls back every window: the hybrid then equals the
     # FP64 judge's window solution there
-    T_u, rec_u = run_hybrid(untrained, k, plan, T0, 256, judge_every=4, tol_K=0.0)
+    # (guard off: the whole-field FP64 redo would hide the networks' own
+    # errors outside the windows, which this compares)
+    T_u, rec_u = run_hybrid(untrained, k, plan, T0, 256, judge_every=4, tol_K=0.0, guard=False)
     assert rec_u["rolled_back"] == rec_u["judged"] == 4
-    T_t, rec_t = run_hybrid(net, k, plan, T0, 256, judge_every=4, tol_K=5.0)
+    T_t, rec_t = run_hybrid(net, k, plan, T0, 256, judge_every=4, tol_K=5.0, guard=False)
     assert rec_t["judged"] == 4
     # the trained network's hybrid field is closer to plain FP64 outside the
     # last window than the untrained one's (no rollback hides it there)
@@ -70,3 +72,33 @@ def test_judge_rolls_back_to_fp64_in_the_window(small_training):
           f"untrained {err_u:.1f} K")
     assert err_t < err_u
     assert torch.isfinite(T_t).all()
+    # with the guard on, the field stays within the maximum-principle range
+    # (its lower end may move down by tol_K per block)
+    T_g, rec_g = run_hybrid(net, k, plan, T0, 256, judge_every=4, tol_K=5.0)
+    assert rec_g["judged"] == 4
+    assert torch.isfinite(T_g).all()
+    assert float(T_g.min()) >= 300.0 - 5.0 * rec_g["judged"], rec_g
+
+
+def test_non_finite_block_is_redone_in_fp64(gpu):
+    """A network whose every parameter is NaN makes the whole field NaN after
+    each block of super-steps; the loop then redoes each block from its start
+    with the FP64 solver over the whole field, so the run ends on the plain
+    FP64 field."""
+    import torch
+    from hedgehog_lpbf_b200.solver import Solver
+    from hedgehog_lpbf_b200.superstep import run_hybrid
+    from hedgehog_lpbf_b200.surrogate import Net, init_params
+    mat, k, plan = _case()
+    net = Net(init_params(0), device="cuda:0")
+    net.set_params(np.full(net.np, np.nan, dtype=np.float32))
+    T0 = np.full(k.nx * k.ny, 300.0)
+    s = Solver(k, Tm=mat.Tm, device="cuda:0")
+    s.advance(plan)
+    T, rec = run_hybrid(net, k, plan, T0, 256, judge_every=4, tol_K=5.0, Tm=mat.Tm)
+    assert rec["full_fp64_blocks"] == rec["judged"] == 4
+    assert torch.isfinite(T).all()
+    # the judge's box solution may replace a window; it differs from the
+    # whole-field solution only through the box edges, far below this bound
+    err = float((T - s.field).abs().max())
+    assert err < 1e-3, err
