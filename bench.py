@@ -723,7 +723,29 @@ def run_b200_arm(args, rank, world, local_rank):
                 "time_steps": STEPS_PER_ITER * (args.warmup + args.steps),
                 "max_abs_err_vs_fp64_K": err32, "target_K": 0.05,
                 "bytes_per_update": 16}
-        del sk, T64
+        del sk
+        # the plain FP32 field (one f32 array, 8 B per update), same plan
+        from hedgehog_lpbf_b200.solver import SolverF32
+        sp = SolverF32(k, device=dev, Tm=mat.Tm, depth=args.depth)
+        for i in range(args.warmup):
+            sp.advance(plan_slice(plan, i), ring)
+        torch.cuda.synchronize()
+        f0.record(stream)
+        for i in range(args.steps):
+            sp.advance(plan_slice(plan, args.warmup + i), ring)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        pms = f0.elapsed_time(f1)
+        errp = float((sp.field64() - T64).abs().max().item())
+        pval = cells * STEPS_PER_ITER * args.steps / (pms * 1e-3) / 1e9
+        hbm = measured_peaks()
+        f32k["plain_f32"] = {
+            "value": pval, "unit": "GCell-updates/s", "ms_per_step": pms / args.steps,
+            "vs_fp64": pval / (value / world), "max_abs_err_vs_fp64_K": errp,
+            "target_K": 0.05, "bytes_per_update": 8,
+            "algorithmic_GBs": pval * 8, "frac_of_hbm": pval * 8 / hbm[0],
+            "hbm_source": hbm[1], "error_word": sp.read_error()}
+        del sp, T64
 
     del s
     # across ranks only on request: that path (NCCL halo exchange) is

@@ -94,6 +94,9 @@ SIGNATURES = {
                                               ctypes.c_size_t, _vp, ctypes.POINTER(ctypes.c_int)]),
     "lpbf_b200_f32k_split": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, _vp]),
     "lpbf_b200_f32k_join": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_size_t, _vp]),
+    "lpbf_b200_advance_f32": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(StepConst), _vp,
+                                             ctypes.c_int, ctypes.POINTER(Opts), _vp, _vp,
+                                             ctypes.c_size_t, _vp, ctypes.POINTER(ctypes.c_int)]),
     "lpbf_b200_advance_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(StepConst), _vp,
                                                  ctypes.c_int, ctypes.POINTER(Opts), _vp, _vp,
                                                  ctypes.POINTER(ctypes.c_int),

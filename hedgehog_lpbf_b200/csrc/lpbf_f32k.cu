@@ -1,7 +1,8 @@
 // SPDX-License-Identifier: 0BSD
 // ---------------------------------------------------------------------------
-// Launch logic and C-ABI of the FP32 compensated step (lpbf_f32k.cuh):
-// lpbf_b200_advance_f32k, lpbf_b200_f32k_split, lpbf_b200_f32k_join.
+// Launch logic and C-ABI of the FP32 steps (lpbf_f32k.cuh): the compensated
+// field (lpbf_b200_advance_f32k, lpbf_b200_f32k_split, lpbf_b200_f32k_join)
+// and the plain f32 field (lpbf_b200_advance_f32).
 // ---------------------------------------------------------------------------
 #include <algorithm>
 #include <cstring>
@@ -30,24 +31,28 @@ FkCoef make_fk(const Coef& c, double T_edge) {
     f.Ta_lo = (float)(Tlin - (double)f.Ta_hi);
     f.Tedge_hi = (float)T_edge;
     f.Tedge_lo = (float)(T_edge - (double)f.Tedge_hi);
+    f.clsTa = (float)((double)f.cls * Tlin);
     return f;
 }
 
-template <int K, bool REDUCE, bool SQ>
+// COMP: the compensated pair field; otherwise the plain f32 field (lo_in and
+// lo_out unused).
+template <int K, bool REDUCE, bool SQ, bool COMP>
 cudaError_t launch_fk(const float* hi_in, const float* lo_in, float* hi_out, float* lo_out,
                       const Coef& c, const FkCoef& f, const LaserSub* las, Partial* ring,
                       Workspace* ws, int rows, cudaStream_t stream) {
-    auto kern = advance_f32k_kernel<K, REDUCE, SQ>;
+    auto kern = advance_f32k_kernel<K, REDUCE, SQ, COMP>;
+    constexpr size_t smem = fk_smem_bytes<COMP>();
     static int occ[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
     if (occ[dev] == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)FK_SMEM_BYTES);
+                                             (int)smem);
         if (e != cudaSuccess) return e;
         int nb = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, ADV_WARPS * 32, FK_SMEM_BYTES);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, ADV_WARPS * 32, smem);
         if (e != cudaSuccess) return e;
         occ[dev] = std::max(1, nb);
     }
@@ -90,30 +95,34 @@ cudaError_t launch_fk(const float* hi_in, const float* lo_in, float* hi_out, flo
     p.tasks = &ws->tasks;
     p.err = &ws->err;
     CUtensorMap mh, ml;
-    if (!tensor_map_f32(hi_in, c.nx, c.ny, ADV_COLS, ADV_R, &mh) ||
-        !tensor_map_f32(lo_in, c.nx, c.ny, ADV_COLS, ADV_R, &ml))
-        return cudaErrorNotSupported;
-    kern<<<grid, ADV_WARPS * 32, FK_SMEM_BYTES, stream>>>(mh, ml, p);
+    if (!tensor_map_f32(hi_in, c.nx, c.ny, ADV_COLS, ADV_R, &mh)) return cudaErrorNotSupported;
+    if (COMP) {
+        if (!tensor_map_f32(lo_in, c.nx, c.ny, ADV_COLS, ADV_R, &ml)) return cudaErrorNotSupported;
+    } else {
+        ml = mh;     // not read by the plain kernel
+    }
+    kern<<<grid, ADV_WARPS * 32, smem, stream>>>(mh, ml, p);
     return cudaGetLastError();
 }
 
+template <bool COMP>
 cudaError_t launch_fk_k(int K, bool reduce, const float* hi_in, const float* lo_in,
                         float* hi_out, float* lo_out, const Coef& c, const FkCoef& f,
                         const LaserSub* las, Partial* ring, Workspace* ws, int rows,
                         cudaStream_t s) {
     // square cells (the f32 coefficients equal) take the one-Laplacian form
     const bool sq = f.ax == f.ay;
-#define LPBF_FK(KK)                                                                         \
-    case KK:                                                                                \
-        if (sq)                                                                             \
-            return reduce ? launch_fk<KK, true, true>(hi_in, lo_in, hi_out, lo_out, c, f, las, \
-                                                      ring, ws, rows, s)                    \
-                          : launch_fk<KK, false, true>(hi_in, lo_in, hi_out, lo_out, c, f,  \
-                                                       las, ring, ws, rows, s);             \
-        return reduce ? launch_fk<KK, true, false>(hi_in, lo_in, hi_out, lo_out, c, f, las,  \
-                                                   ring, ws, rows, s)                       \
-                      : launch_fk<KK, false, false>(hi_in, lo_in, hi_out, lo_out, c, f, las, \
-                                                    ring, ws, rows, s);
+#define LPBF_FK(KK)                                                                          \
+    case KK:                                                                                 \
+        if (sq)                                                                              \
+            return reduce ? launch_fk<KK, true, true, COMP>(hi_in, lo_in, hi_out, lo_out, c, \
+                                                            f, las, ring, ws, rows, s)       \
+                          : launch_fk<KK, false, true, COMP>(hi_in, lo_in, hi_out, lo_out, c, \
+                                                             f, las, ring, ws, rows, s);     \
+        return reduce ? launch_fk<KK, true, false, COMP>(hi_in, lo_in, hi_out, lo_out, c, f,  \
+                                                         las, ring, ws, rows, s)             \
+                      : launch_fk<KK, false, false, COMP>(hi_in, lo_in, hi_out, lo_out, c, f, \
+                                                          las, ring, ws, rows, s);
     switch (K) {
         LPBF_FK(1)
         LPBF_FK(2)
@@ -203,12 +212,55 @@ int lpbf_b200_advance_f32k(float* hi_a, float* lo_a, float* hi_b, float* lo_b,
         LaserSub las[KMAX];
         for (int t = 0; t < kk; ++t)
             las[t] = make_laser(*k, plan[s0 + t].x_l, plan[s0 + t].y_l, plan[s0 + t].q_scale);
-        const cudaError_t e = launch_fk_k(kk, ring != nullptr, ch, cl, nh, nl, c, f, las,
-                                          ring ? ring + s0 : nullptr, ws, opts->rows, stream);
+        const cudaError_t e = launch_fk_k<true>(kk, ring != nullptr, ch, cl, nh, nl, c, f, las,
+                                                ring ? ring + s0 : nullptr, ws, opts->rows,
+                                                stream);
         if (e == cudaErrorNotSupported) return LPBF_ERR_TMA;
         if (e != cudaSuccess) return LPBF_ERR_CUDA;
         std::swap(ch, nh);
         std::swap(cl, nl);
+        in_b ^= 1;
+    }
+    *result_in_b = in_b;
+    return LPBF_OK;
+}
+
+int lpbf_b200_advance_f32(float* T_a, float* T_b, const StepConst* k, const lpbf_tick* plan,
+                          int n_steps, const lpbf_b200_opts* opts, Partial* ring, void* work,
+                          size_t work_bytes, cudaStream_t stream, int* result_in_b) {
+    NvtxRange nvtx_range("lpbf_b200_advance_f32");
+    if (!k || k->nx < 2 || k->ny < 1 || !opts || !T_a || !T_b || n_steps < 0 ||
+        (n_steps > 0 && !plan) || !result_in_b)
+        return LPBF_ERR_ARG;
+    if (opts->bc != 0 && opts->bc != 1) return LPBF_ERR_ARG;
+    if (opts->phys != 0) return LPBF_ERR_UNSUPPORTED;
+    if (k->nx % 4 != 0 || !aligned16(T_a) || !aligned16(T_b)) return LPBF_ERR_UNSUPPORTED;
+    const size_t N = (size_t)k->nx * k->ny;
+    if (T_a < T_b + N && T_b < T_a + N) return LPBF_ERR_ARG;
+    Workspace* ws = static_cast<Workspace*>(work);
+    if (!ws || work_bytes < sizeof(Workspace)) return LPBF_ERR_WORKSPACE;
+
+    int depth = opts->depth;
+    if (depth <= 0) {
+        const long long n = (long long)N;
+        depth = (n >= (1ll << 22)) ? 3 : (n >= (1ll << 18)) ? 2 : 1;
+    }
+    depth = std::min(std::max(depth, 1), 4);
+    const Coef c = make_coef(*k, opts->bc, opts->T_edge, opts->Tm);
+    const FkCoef f = make_fk(c, opts->T_edge);
+    float *cur = T_a, *nxt = T_b;
+    int in_b = 0;
+    for (int s0 = 0; s0 < n_steps; s0 += depth) {
+        const int kk = std::min(depth, n_steps - s0);
+        LaserSub las[KMAX];
+        for (int t = 0; t < kk; ++t)
+            las[t] = make_laser(*k, plan[s0 + t].x_l, plan[s0 + t].y_l, plan[s0 + t].q_scale);
+        const cudaError_t e = launch_fk_k<false>(kk, ring != nullptr, cur, nullptr, nxt, nullptr,
+                                                 c, f, las, ring ? ring + s0 : nullptr, ws,
+                                                 opts->rows, stream);
+        if (e == cudaErrorNotSupported) return LPBF_ERR_TMA;
+        if (e != cudaSuccess) return LPBF_ERR_CUDA;
+        std::swap(cur, nxt);
         in_b ^= 1;
     }
     *result_in_b = in_b;

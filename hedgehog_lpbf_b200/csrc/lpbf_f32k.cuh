@@ -19,6 +19,11 @@
 // Structure (warp tasks, lanes, TMA pipeline, wavefront, fast/general boxes,
 // two-tier reduction) follows lpbf_advance.cuh; the per-step Partials are
 // computed on T = (double)hi + (double)lo, which is exact.
+//
+// The same kernel with COMP = false is the plain FP32 field: one f32 array,
+// each step's update rounded once (the FP64 step's fused form in f32, the
+// source still evaluated in FP64), 8 bytes per cell-update; no lo array is
+// loaded, staged, shuffled or stored.
 // ---------------------------------------------------------------------------
 #pragma once
 #include <stddef.h>
@@ -27,10 +32,14 @@
 
 namespace lpbf_b200 {
 
-constexpr int FK_STAGE_FLOATS = 2 * ADV_R * ADV_COLS;      // hi box then lo box
-constexpr size_t FK_SMEM_BYTES =
-    size_t(ADV_WARPS) * ADV_S * FK_STAGE_FLOATS * sizeof(float)
-    + size_t(ADV_WARPS) * ADV_S * sizeof(uint64_t);
+// floats per TMA stage: the hi box, then (compensated field) the lo box
+template <bool COMP>
+constexpr int fk_stage_floats() { return (COMP ? 2 : 1) * ADV_R * ADV_COLS; }
+template <bool COMP>
+constexpr size_t fk_smem_bytes() {
+    return size_t(ADV_WARPS) * ADV_S * fk_stage_floats<COMP>() * sizeof(float)
+           + size_t(ADV_WARPS) * ADV_S * sizeof(uint64_t);
+}
 
 // 16-byte store issued under a predicate (no branch).  It carries a
 // "memory" clobber: the exact reduction reads level-K values back from the
@@ -46,6 +55,7 @@ struct FkCoef {
     float ax, ay, cls, crad;
     float Ta_hi, Ta_lo, Ta4;       // linear-loss reference T as a pair; Ta4 = f4(Tamb)
     float Tedge_hi, Tedge_lo;
+    float clsTa;                   // c_ls * (linear-loss reference T), rounded once
 };
 
 struct FkParams {
@@ -107,14 +117,40 @@ __device__ __forceinline__ void fk_cell(float th, float tl, float Lh, float Ll, 
     ol = __fsub_rn(lo, __fsub_rn(oh, s));
 }
 
+// One plain f32 cell update: the FP64 step's form in f32.  T^4 - Ta^4 and
+// c_ls T - c_ls Ta are each one fused multiply-add and the loss enters the
+// increment's fused chain (SQ: one Laplacian (R + L) + (U + D) - 4T).  The
+// Laplacian of a uniform field is exactly zero and its loss at Tamb far below
+// half an ulp of T, so a uniform field at Tamb stays exactly uniform.
+// SRC: the cell's source increment S is added to the net change before T.
+template <bool SQ, bool SRC>
+__device__ __forceinline__ float f32_cell(float t, float L, float R, float U, float D, float S,
+                                          const FkCoef& f) {
+    const float t2 = __fmul_rn(t, t);
+    const float e4 = fmaf(t2, t2, -f.Ta4);
+    const float loss = fmaf(f.crad, e4, fmaf(f.cls, t, -f.clsTa));
+    float net;
+    if constexpr (SQ) {
+        const float lap = fmaf(-4.0f, t, __fadd_rn(__fadd_rn(R, L), __fadd_rn(U, D)));
+        net = fmaf(f.ax, lap, -loss);
+    } else {
+        const float lx = fmaf(-2.0f, t, __fadd_rn(R, L));
+        const float ly = fmaf(-2.0f, t, __fadd_rn(U, D));
+        net = fmaf(f.ax, lx, fmaf(f.ay, ly, -loss));
+    }
+    if constexpr (SRC) net = __fadd_rn(net, S);
+    return __fadd_rn(t, net);
+}
+
 // (a.hi, a.lo) > (b.hi, b.lo) for canonical pairs.
 __device__ __forceinline__ bool fk_gt(float ah, float al, float bh, float bl) {
     return ah > bh || (ah == bh && al > bl);
 }
 
-template <int K, bool REDUCE, bool SQ>
+template <int K, bool REDUCE, bool SQ, bool COMP>
 struct FkStrip {
     static constexpr int V = ADV_V;
+    static constexpr int STAGE = fk_stage_floats<COMP>();
 
     const FkParams& p;
     const CUtensorMap* map_hi;
@@ -159,10 +195,11 @@ struct FkStrip {
     __device__ __forceinline__ void issue(int b) {
         const uint32_t g = gbox + b;
         const int st = g % ADV_S;
-        float* dst = stages + st * FK_STAGE_FLOATS;
-        mbar_expect_tx(&bars[st], FK_STAGE_FLOATS * sizeof(float));
+        float* dst = stages + st * STAGE;
+        mbar_expect_tx(&bars[st], STAGE * sizeof(float));
         tma_load_2d(dst, map_hi, xs, jy0 + b * ADV_R, &bars[st]);
-        tma_load_2d(dst + ADV_R * ADV_COLS, map_lo, xs, jy0 + b * ADV_R, &bars[st]);
+        if constexpr (COMP)
+            tma_load_2d(dst + ADV_R * ADV_COLS, map_lo, xs, jy0 + b * ADV_R, &bars[st]);
         issued = b + 1;
     }
 
@@ -211,7 +248,7 @@ struct FkStrip {
                     failed = true;
                     break;
                 }
-                st = stages + sidx * FK_STAGE_FLOATS;
+                st = stages + sidx * STAGE;
             }
             // mirror-edge strips too: row_update patches the edge cells'
             // outer neighbours itself (nx a multiple of 4: whole lanes)
@@ -249,9 +286,12 @@ struct FkStrip {
     template <int P>
     __device__ __forceinline__ void load_row0(const float* st) {
         const float4 h = *reinterpret_cast<const float4*>(st + P * ADV_COLS + 4 * lane);
-        const float4 l = *reinterpret_cast<const float4*>(st + (ADV_R + P) * ADV_COLS + 4 * lane);
         wh0[P][0] = h.x; wh0[P][1] = h.y; wh0[P][2] = h.z; wh0[P][3] = h.w;
-        wl0[P][0] = l.x; wl0[P][1] = l.y; wl0[P][2] = l.z; wl0[P][3] = l.w;
+        if constexpr (COMP) {
+            const float4 l =
+                *reinterpret_cast<const float4*>(st + (ADV_R + P) * ADV_COLS + 4 * lane);
+            wl0[P][0] = l.x; wl0[P][1] = l.y; wl0[P][2] = l.z; wl0[P][3] = l.w;
+        }
     }
 
     template <int T>
@@ -263,27 +303,46 @@ struct FkStrip {
         if constexpr (T == 0) return wl0; else return wl[T - 1];
     }
 
-    // One row of level T from the three rows (up, centre, down) of level T-1.
+    // One row of level T from the three rows (up, centre, down) of level T-1
+    // (plain field: the lo rows are not read and ol is not written).
     __device__ __forceinline__ void row_update(const float* uh, const float* ul, const float* ch,
                                                const float* cl, const float* dh, const float* dl,
                                                const float* S, float* oh, float* ol) {
-        const float Lh0 = __shfl_up_sync(0xffffffffu, ch[V - 1], 1);
-        const float Ll0 = __shfl_up_sync(0xffffffffu, cl[V - 1], 1);
-        const float Rh3 = __shfl_down_sync(0xffffffffu, ch[0], 1);
-        const float Rl3 = __shfl_down_sync(0xffffffffu, cl[0], 1);
-        float Lh[V] = {Lh0, ch[0], ch[1], ch[2]}, Ll[V] = {Ll0, cl[0], cl[1], cl[2]};
-        float Rh[V] = {ch[1], ch[2], ch[3], Rh3}, Rl[V] = {cl[1], cl[2], cl[3], Rl3};
-        if (edge) {
+        if constexpr (!COMP) {
+            const float L0 = __shfl_up_sync(0xffffffffu, ch[V - 1], 1);
+            const float R3 = __shfl_down_sync(0xffffffffu, ch[0], 1);
+            float L[V] = {L0, ch[0], ch[1], ch[2]};
+            float R[V] = {ch[1], ch[2], ch[3], R3};
+            if (edge) {
 #pragma unroll
-            for (int v = 0; v < V; ++v) {
-                if (xl + v == 0) { Lh[v] = ch[v]; Ll[v] = cl[v]; }
-                if (xl + v == p.c.nx - 1) { Rh[v] = ch[v]; Rl[v] = cl[v]; }
+                for (int v = 0; v < V; ++v) {
+                    if (xl + v == 0) L[v] = ch[v];
+                    if (xl + v == p.c.nx - 1) R[v] = ch[v];
+                }
             }
-        }
 #pragma unroll
-        for (int v = 0; v < V; ++v)
-            fk_cell<SQ>(ch[v], cl[v], Lh[v], Ll[v], Rh[v], Rl[v], uh[v], ul[v], dh[v], dl[v],
-                    S ? S[v] : 0.0f, p.f, oh[v], ol[v]);
+            for (int v = 0; v < V; ++v)
+                oh[v] = S ? f32_cell<SQ, true>(ch[v], L[v], R[v], uh[v], dh[v], S[v], p.f)
+                          : f32_cell<SQ, false>(ch[v], L[v], R[v], uh[v], dh[v], 0.0f, p.f);
+        } else {
+            const float Lh0 = __shfl_up_sync(0xffffffffu, ch[V - 1], 1);
+            const float Ll0 = __shfl_up_sync(0xffffffffu, cl[V - 1], 1);
+            const float Rh3 = __shfl_down_sync(0xffffffffu, ch[0], 1);
+            const float Rl3 = __shfl_down_sync(0xffffffffu, cl[0], 1);
+            float Lh[V] = {Lh0, ch[0], ch[1], ch[2]}, Ll[V] = {Ll0, cl[0], cl[1], cl[2]};
+            float Rh[V] = {ch[1], ch[2], ch[3], Rh3}, Rl[V] = {cl[1], cl[2], cl[3], Rl3};
+            if (edge) {
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    if (xl + v == 0) { Lh[v] = ch[v]; Ll[v] = cl[v]; }
+                    if (xl + v == p.c.nx - 1) { Rh[v] = ch[v]; Rl[v] = cl[v]; }
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < V; ++v)
+                fk_cell<SQ>(ch[v], cl[v], Lh[v], Ll[v], Rh[v], Rl[v], uh[v], ul[v], dh[v],
+                            dl[v], S ? S[v] : 0.0f, p.f, oh[v], ol[v]);
+        }
     }
 
     template <int P>
@@ -327,11 +386,17 @@ struct FkStrip {
                 float (&al)[3][V] = winl<T - 1>();
                 if (r == 0) {
 #pragma unroll
-                    for (int v = 0; v < V; ++v) { ah[su][v] = ah[sc][v]; al[su][v] = al[sc][v]; }
+                    for (int v = 0; v < V; ++v) {
+                        ah[su][v] = ah[sc][v];
+                        if constexpr (COMP) al[su][v] = al[sc][v];
+                    }
                 }
                 if (r == ny - 1) {
 #pragma unroll
-                    for (int v = 0; v < V; ++v) { ah[sd][v] = ah[sc][v]; al[sd][v] = al[sc][v]; }
+                    for (int v = 0; v < V; ++v) {
+                        ah[sd][v] = ah[sc][v];
+                        if constexpr (COMP) al[sd][v] = al[sc][v];
+                    }
                 }
                 float oh[V], ol[V];
                 if (p.c.bc == 1 && (r == 0 || r == ny - 1)) {
@@ -371,7 +436,10 @@ struct FkStrip {
             float (&bh)[3][V] = winh<T>();
             float (&bl)[3][V] = winl<T>();
 #pragma unroll
-            for (int v = 0; v < V; ++v) { bh[SC][v] = oh[v]; bl[SC][v] = ol[v]; }
+            for (int v = 0; v < V; ++v) {
+                bh[SC][v] = oh[v];
+                if constexpr (COMP) bl[SC][v] = ol[v];
+            }
         } else {
             // nx is a multiple of 4 (checked on entry): an owned lane's four
             // cells are in the field and 16-byte aligned; the stores are
@@ -379,7 +447,7 @@ struct FkStrip {
             const size_t off = (size_t)r * p.c.nx + xl;
             const bool st = owned_row && owned_lane();
             st_global_v4f_pred(p.Thi_out + off, oh, st);
-            st_global_v4f_pred(p.Tlo_out + off, ol, st);
+            if constexpr (COMP) st_global_v4f_pred(p.Tlo_out + off, ol, st);
         }
         if constexpr (REDUCE) {
             bool h = hit[T - 1];
@@ -387,7 +455,10 @@ struct FkStrip {
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 const bool ok = ol_ok && (full || xl + v < p.c.nx);
-                h = h | (ok && fk_gt(oh[v], ol[v], thr_h[T - 1], thr_l[T - 1]));
+                if constexpr (COMP)
+                    h = h | (ok && fk_gt(oh[v], ol[v], thr_h[T - 1], thr_l[T - 1]));
+                else
+                    h = h | (ok && oh[v] > thr_h[T - 1]);
             }
             hit[T - 1] = h;
         }
@@ -400,11 +471,17 @@ struct FkStrip {
         for (int t = 0; t < K; ++t) {
             double a = s_tmx[t][lane];
             a = (a < p.c.Tm) ? a : p.c.Tm;
-            // the largest pair not above a: compare strictly against it
-            const float h = (float)a;
-            const float l = (float)(a - (double)h);
-            thr_h[t] = ol ? h : INFINITY;
-            thr_l[t] = ol ? l : 0.0f;
+            if constexpr (COMP) {
+                // the largest pair not above a: compare strictly against it
+                const float h = (float)a;
+                const float l = (float)(a - (double)h);
+                thr_h[t] = ol ? h : INFINITY;
+                thr_l[t] = ol ? l : 0.0f;
+            } else {
+                // the largest float not above a: a float cell exceeds it
+                // exactly when it exceeds a
+                thr_h[t] = ol ? __double2float_rd(a) : INFINITY;
+            }
         }
     }
 
@@ -420,16 +497,23 @@ struct FkStrip {
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
                     d[v] = (s == 0) ? winh<T>()[0][v] : (s == 1) ? winh<T>()[1][v] : winh<T>()[2][v];
-                    d[V + v] = (s == 0) ? winl<T>()[0][v] : (s == 1) ? winl<T>()[1][v] : winl<T>()[2][v];
+                    if constexpr (COMP)
+                        d[V + v] = (s == 0) ? winl<T>()[0][v]
+                                 : (s == 1) ? winl<T>()[1][v] : winl<T>()[2][v];
                 }
             }
         }
     }
 
     __device__ __forceinline__ double value_at(int t, int P, int r, int v) const {
-        if (t < K) return (double)s_box[P][lane][v] + (double)s_box[P][lane][V + v];
         const size_t off = (size_t)r * p.c.nx + xl + v;
-        return (double)p.Thi_out[off] + (double)p.Tlo_out[off];
+        if constexpr (COMP) {
+            if (t < K) return (double)s_box[P][lane][v] + (double)s_box[P][lane][V + v];
+            return (double)p.Thi_out[off] + (double)p.Tlo_out[off];
+        } else {
+            if (t < K) return (double)s_box[P][lane][v];
+            return (double)p.Thi_out[off];
+        }
     }
 
     __device__ __forceinline__ void exact_level(int t, int j) {
@@ -486,7 +570,7 @@ struct FkStrip {
     }
 };
 
-template <int K, bool REDUCE, bool SQ>
+template <int K, bool REDUCE, bool SQ, bool COMP>
 __global__ void __launch_bounds__(ADV_WARPS * 32, AdvOcc<K>::min_ctas)
 advance_f32k_kernel(const __grid_constant__ CUtensorMap map_hi,
                     const __grid_constant__ CUtensorMap map_lo,
@@ -500,9 +584,10 @@ advance_f32k_kernel(const __grid_constant__ CUtensorMap map_hi,
     __shared__ __align__(16) float s_box[ADV_WARPS][3][32][2 * ADV_V];
 
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float* stages = reinterpret_cast<float*>(smem) + wid * (ADV_S * FK_STAGE_FLOATS);
+    constexpr int STAGE = fk_stage_floats<COMP>();
+    float* stages = reinterpret_cast<float*>(smem) + wid * (ADV_S * STAGE);
     uint64_t* bars = reinterpret_cast<uint64_t*>(
-        smem + size_t(ADV_WARPS) * ADV_S * FK_STAGE_FLOATS * sizeof(float)) + wid * ADV_S;
+        smem + size_t(ADV_WARPS) * ADV_S * STAGE * sizeof(float)) + wid * ADV_S;
     if (lane == 0) {
         for (int s = 0; s < ADV_S; ++s) mbar_init(&bars[s], 1);
         fence_mbar_init();
@@ -510,7 +595,7 @@ advance_f32k_kernel(const __grid_constant__ CUtensorMap map_hi,
     }
     __syncwarp();
 
-    FkStrip<K, REDUCE, SQ> ws(p, &map_hi, &map_lo, stages, bars, lane, s_tmx[wid], s_arg[wid],
+    FkStrip<K, REDUCE, SQ, COMP> ws(p, &map_hi, &map_lo, stages, bars, lane, s_tmx[wid], s_arg[wid],
                           s_ymn[wid], s_ymx[wid], s_box[wid]);
     for (;;) {
         unsigned int t = 0;

@@ -246,3 +246,67 @@ class SolverF32K:
                                                     self.lo[self.cur].data_ptr(), out.data_ptr(),
                                                     n, _stream_handle(None)), "f32k_join")
         return out.view(self.ny, self.nx)
+
+
+class SolverF32:
+    """The plain FP32 field (one f32 array, each step's update rounded once)
+    with the same plan API as Solver; ``field`` is the f32 field and
+    ``field64()`` its FP64 copy."""
+
+    def __init__(self, k: StepConst, *, bc: int = 0, T_edge: float = 300.0, Tm: float = 1609.0,
+                 depth: int = 0, rows: int = 0, device: torch.device | str | None = None,
+                 T0: float | np.ndarray | None = None):
+        self.lib = _lib.lib()
+        self.k = StepConst.from_buffer_copy(bytes(k))
+        self.nx, self.ny = k.nx, k.ny
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        self.opts = _lib.Opts(phys=0, bc=bc, T_edge=T_edge, Tm=Tm, depth=depth, rows=rows)
+        n = self.nx * self.ny
+        self.bufs = [torch.empty(n, dtype=torch.float32, device=self.device) for _ in range(2)]
+        self.cur = 0
+        nbytes = self.lib.lpbf_b200_workspace_bytes()
+        self.work = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.lpbf_b200_workspace_init(self.work.data_ptr(), nbytes,
+                                                         _stream_handle(None)), "workspace_init")
+        self.set_field(k.Tamb if T0 is None else T0)
+
+    def set_field(self, T0) -> None:
+        if np.isscalar(T0):
+            self.bufs[self.cur].fill_(float(T0))
+        else:
+            src = torch.as_tensor(np.asarray(T0, dtype=np.float64).ravel()).to(self.device)
+            self.bufs[self.cur].copy_(src)        # rounded to nearest
+
+    @property
+    def field(self) -> torch.Tensor:
+        return self.bufs[self.cur].view(self.ny, self.nx)
+
+    def field64(self) -> torch.Tensor:
+        return self.field.double()
+
+    def new_ring(self, n_steps: int) -> torch.Tensor:
+        return torch.zeros(n_steps * 24, dtype=torch.uint8, device=self.device)
+
+    def read_error(self) -> int:
+        err = ctypes.c_uint(0)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.lpbf_b200_read_error(self.work.data_ptr(), _stream_handle(None),
+                                                     ctypes.byref(err)), "read_error")
+        return err.value
+
+    def advance(self, plan: np.ndarray, ring: torch.Tensor | None = None,
+                stream: torch.cuda.Stream | None = None) -> None:
+        plan = np.ascontiguousarray(plan, dtype=TICK_DTYPE)
+        n = len(plan)
+        in_b = ctypes.c_int(0)
+        a, b = self.cur, 1 - self.cur
+        with torch.cuda.device(self.device):
+            st = self.lib.lpbf_b200_advance_f32(
+                self.bufs[a].data_ptr(), self.bufs[b].data_ptr(), ctypes.byref(self.k),
+                plan.ctypes.data if n else None, n, ctypes.byref(self.opts),
+                ring.data_ptr() if ring is not None else None, self.work.data_ptr(),
+                self.work.numel(), _stream_handle(stream), ctypes.byref(in_b))
+        _lib.check(st, "lpbf_b200_advance_f32")
+        if in_b.value:
+            self.cur = 1 - self.cur

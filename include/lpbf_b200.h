@@ -143,6 +143,17 @@ int lpbf_b200_f32k_split(const double* T, float* hi, float* lo, size_t n, cudaSt
 int lpbf_b200_f32k_join(const float* hi, const float* lo, double* T, size_t n,
                         cudaStream_t stream);
 
+/* Plain FP32 field (no reference counterpart): one f32 array, each step's
+ * update rounded once (the FP64 step's operations in f32; the Gaussian source
+ * evaluated in FP64 and rounded), 8 bytes per cell-update against 16 for the
+ * FP64 and compensated fields.  Per-step Partials are reduced on the f32
+ * values (exactly, in FP64).  T_a holds the start field, T_b the other half
+ * of the ping-pong pair; *result_in_b, requirements and workspace as for
+ * lpbf_b200_advance_f32k. */
+int lpbf_b200_advance_f32(float* T_a, float* T_b, const StepConst* k, const lpbf_tick* plan,
+                          int n_steps, const lpbf_b200_opts* opts, Partial* ring, void* work,
+                          size_t work_bytes, cudaStream_t stream, int* result_in_b);
+
 /* No counterpart in the reference.  lpbf_b200_advance without a workspace,
  * for callers that cannot allocate device memory: code running inside a
  * device-memory budget fixed at start-up, bindings that only pass raw device
