@@ -65,9 +65,12 @@ cudaError_t launch_fk(const float* hi_in, const float* lo_in, float* hi_out, flo
     laser_band(c, las, K, &p.band_lo, &p.band_hi, &p.bandx_lo, &p.bandx_hi);
     p.nstrips = (c.nx + ADV_WOUT - 1) / ADV_WOUT;
     int H = rows;
-    if (H <= 0) {   // about three tasks per resident warp, 12..48 rows (48 measured best)
+    if (H <= 0) {
+        // about three tasks per resident warp, 12..48 rows for the pairs and
+        // 12..64 for the plain field (the best measured at 8192^2, depth 3:
+        // pairs 48; plain 64, 1045 GCell-updates/s against 1008 with 48)
         const long long want = (long long)c.ny * p.nstrips / (3ll * resident * ADV_WARPS);
-        H = (int)std::max(12ll, std::min(48ll, want));
+        H = (int)std::max(12ll, std::min(COMP ? 48ll : 64ll, want));
     }
     p.H = std::max(std::min(H, c.ny), 1);
     // rows whose tasks (owned rows +- K) reach the source band: 8-row tasks
