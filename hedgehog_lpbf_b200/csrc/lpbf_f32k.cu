@@ -66,11 +66,10 @@ cudaError_t launch_fk(const float* hi_in, const float* lo_in, float* hi_out, flo
     p.nstrips = (c.nx + ADV_WOUT - 1) / ADV_WOUT;
     int H = rows;
     if (H <= 0) {
-        // about three tasks per resident warp, 12..48 rows for the pairs and
-        // 12..64 for the plain field (the best measured at 8192^2, depth 3:
-        // pairs 48; plain 64, 1045 GCell-updates/s against 1008 with 48)
+        // about three tasks per resident warp, 12..48 rows (48 measured best
+        // at 8192^2, depth 3, for both fields over the bench raster)
         const long long want = (long long)c.ny * p.nstrips / (3ll * resident * ADV_WARPS);
-        H = (int)std::max(12ll, std::min(COMP ? 48ll : 64ll, want));
+        H = (int)std::max(12ll, std::min(48ll, want));
     }
     p.H = std::max(std::min(H, c.ny), 1);
     // rows whose tasks (owned rows +- K) reach the source band: 8-row tasks
@@ -188,7 +187,8 @@ int lpbf_b200_advance_f32k(float* hi_a, float* lo_a, float* hi_b, float* lo_b,
         n_steps < 0 || (n_steps > 0 && !plan) || !result_in_b)
         return LPBF_ERR_ARG;
     if (opts->bc != 0 && opts->bc != 1) return LPBF_ERR_ARG;
-    if (opts->phys != 0) return LPBF_ERR_UNSUPPORTED;
+    if (opts->phys != 0 && opts->phys != 1) return LPBF_ERR_ARG;
+    if (opts->phys == 1) return LPBF_ERR_UNSUPPORTED;     // baseline physics only
     if (k->nx % 4 != 0 || !aligned16(hi_a) || !aligned16(lo_a) || !aligned16(hi_b) ||
         !aligned16(lo_b))
         return LPBF_ERR_UNSUPPORTED;
@@ -236,7 +236,8 @@ int lpbf_b200_advance_f32(float* T_a, float* T_b, const StepConst* k, const lpbf
         (n_steps > 0 && !plan) || !result_in_b)
         return LPBF_ERR_ARG;
     if (opts->bc != 0 && opts->bc != 1) return LPBF_ERR_ARG;
-    if (opts->phys != 0) return LPBF_ERR_UNSUPPORTED;
+    if (opts->phys != 0 && opts->phys != 1) return LPBF_ERR_ARG;
+    if (opts->phys == 1) return LPBF_ERR_UNSUPPORTED;     // baseline physics only
     if (k->nx % 4 != 0 || !aligned16(T_a) || !aligned16(T_b)) return LPBF_ERR_UNSUPPORTED;
     const size_t N = (size_t)k->nx * k->ny;
     if (T_a < T_b + N && T_b < T_a + N) return LPBF_ERR_ARG;

@@ -45,6 +45,27 @@ def test_host_only_entry_points():
     assert L.lpbf_b200_advance(None, None, None, None, 0, None, None, None, 0, None, None) == -1
 
 
+def test_fp32_entry_points_validate_physics_before_any_cuda_call():
+    """As lpbf_b200_advance: phys other than 0/1 is an invalid argument, phys 1
+    a valid request these entry points do not implement.  The buffers are
+    host addresses the calls must not touch (rejected before any launch)."""
+    from hedgehog_lpbf_b200.params import StepConst
+    L = _lib.lib()
+    k = StepConst()
+    k.nx, k.ny = 64, 64
+    bufs = [ctypes.create_string_buffer(64) for _ in range(4)]
+    a = [ctypes.addressof(b) for b in bufs]
+    in_b = ctypes.c_int(0)
+    for phys, want in ((1, -2), (2, -1), (-1, -1)):
+        o = _lib.Opts(phys=phys, bc=0, T_edge=300.0, Tm=1609.0, depth=3, rows=0)
+        st = L.lpbf_b200_advance_f32(a[0], a[1], ctypes.byref(k), None, 0, ctypes.byref(o),
+                                     None, None, 0, None, ctypes.byref(in_b))
+        assert st == want, ("f32", phys, st)
+        st = L.lpbf_b200_advance_f32k(a[0], a[1], a[2], a[3], ctypes.byref(k), None, 0,
+                                      ctypes.byref(o), None, None, 0, None, ctypes.byref(in_b))
+        assert st == want, ("f32k", phys, st)
+
+
 @pytest.mark.parametrize("lang", ["c", "c++"])
 def test_headers_compile_and_link(tmp_path, lang):
     src = tmp_path / ("t.c" if lang == "c" else "t.cpp")
